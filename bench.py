@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark: seconds per FUGAL alignment on one B200 (and N independent replicas).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload er32768] [--stream-dtype bf16]
+    python bench.py --impl reference ...     # the reference's CPU path, timed on this host
+
+A step is one whole alignment of the workload's graph pair: node features,
+15 x 10 Frank-Wolfe steps (gradient, log-domain Sinkhorn solve of up to 500
+sweeps, update) and the rounding, on inputs already resident in HBM (`value`).
+`e2e` runs the same alignment through the public ``cugal()`` call from the
+networkx graphs on the host, including the host-to-device copies of the edge
+lists and the device-to-host copy of the result (P and the mapping).
+
+With N > 1 (torchrun), every rank aligns its own copy of the workload (replicas;
+the alignment path has no exchange step), timing is the max over ranks and
+`value` is seconds per step, i.e. per N alignments (weak scaling).
+
+The JSON line also carries the roofline of the dominant kernel (the BF16 sweep:
+algorithmic bytes = one read of the n x ld 16-bit cost per launch, averaged over
+the launches of the timed region with CUDA events on the launch stream), the
+host CPU baseline (the reference's FP64 CPU Sinkhorn iteration timed on a block
+of rows, extrapolated), SM clocks sampled during the timed region, and the
+number of this library's kernel launches in the timed region.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "align secs & Sinkhorn HBM GB/s at n=32768: BF16-cost vs FP32 path, same accuracy"
+UNIT = "s/alignment"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="er32768")
+    ap.add_argument("--n", type=int, default=None, help="override the workload size")
+    ap.add_argument("--stream-dtype", choices=["bf16", "fp16", "fp32"], default="bf16")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--iter-count", type=int, default=None, help="override the lambda steps (smoke runs)")
+    ap.add_argument("--sinkhorn-iterations", type=int, default=None)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ----------------------------------------------------------------- distributed
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def dist_init(world: int, backend: str):
+    if world > 1 and not torch.distributed.is_initialized():
+        import datetime
+        torch.distributed.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+
+
+def barrier(world: int):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(x: float, world: int, device) -> float:
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        power = [float(r[3]) for r in rows if r[3].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(rows), "power_w_max": max(power) if power else None, "reasons": reasons}
+
+
+# ----------------------------------------------------------------- CPU baseline
+def cpu_sweep_seconds(n: int, budget_s: float) -> tuple[float, int, str]:
+    """Seconds per Sinkhorn iteration of the reference CPU path at size n.
+
+    Restates cugal/sinkhorn.py:108-111 (torch FP64: a column logsumexp and a row
+    logsumexp over K + potentials) on a block of rows of an n-column cost, all
+    host threads, and scales the per-row time to n rows.  Uses the oracle's
+    module only for its shapes; the arithmetic is torch's, as in the reference."""
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    rows = max(64, min(n, 2048))
+    g = torch.Generator().manual_seed(0)
+    K = -torch.rand((rows, n), generator=g, dtype=torch.float64) * 4000.0
+    u = torch.zeros(rows, dtype=torch.float64)
+    v = torch.zeros(n, dtype=torch.float64)
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or len(times) < 2:
+        t0 = time.perf_counter()
+        v = -torch.logsumexp(K + u[:, None], 0)
+        u = -torch.logsumexp(K + v[None, :], 1)
+        times.append(time.perf_counter() - t0)
+    per_iter = statistics.median(times[1:] if len(times) > 2 else times) * (n / rows)
+    sample = (f"{len(times)} reference CPU Sinkhorn iterations (torch FP64 column+row logsumexp, "
+              f"cugal/sinkhorn.py:108-111) on a {rows}x{n} block, scaled to {n} rows")
+    return per_iter, threads, sample
+
+
+def cpu_alignment_seconds(n: int, solves: int, sweeps_per_solve: float, budget_s: float):
+    per_iter, threads, sample = cpu_sweep_seconds(n, budget_s)
+    total = per_iter * sweeps_per_solve * solves
+    sample += f"; alignment = {solves} solves x {sweeps_per_solve:g} iterations (Sinkhorn only, a lower bound)"
+    return total, threads, sample
+
+
+# ----------------------------------------------------------------- measurement
+def load_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(n: int, ld: int):
+    """DRAM bytes per 16-bit sweep launch from the committed ncu summary (scaled by rows x ld), or None."""
+    f = ROOT / "profiles" / "sweep_bf16_traffic.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    return d["dram_bytes_per_launch"] * (n * ld) / (d["n"] * d["ld"])
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from cugal_b200.synthetic import WORKLOADS
+    w = WORKLOADS[args.workload]
+    n = args.n or w.n
+    iters = args.iter_count or w.iter_count
+    solves = iters * 10
+    sweeps = args.sinkhorn_iterations or 500
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sweep_seconds(n, min(2.0, args.cpu_seconds / 4))
+    threads, sample = 0, ""
+    for _ in range(args.steps):
+        v, threads, sample = cpu_alignment_seconds(n, solves, sweeps, args.cpu_seconds / max(1, args.steps))
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "n": n, "solves": solves, "sweeps_per_solve": sweeps},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    world, rank, local = dist_env()
+    dist_init(world, "nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from cugal_b200 import Profile, cugal
+    from cugal_b200 import _native as N
+    from cugal_b200.adjacency import Adjacency, edge_array
+    from cugal_b200.pred import align
+    from cugal_b200.sinkhorn import padded_ld
+    from cugal_b200.synthetic import config_for, make_pair, node_accuracy
+
+    sdt = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": None}[args.stream_dtype]
+    src, tgt, perm, w = make_pair(args.workload, n=args.n)
+    over = {"stream_dtype": sdt, "device": f"cuda:{local}"}
+    if args.iter_count:
+        over["iter_count"] = args.iter_count
+    if args.sinkhorn_iterations:
+        over["sinkhorn_iterations"] = args.sinkhorn_iterations
+    config = config_for(w, **over)
+    n = src.number_of_nodes()
+    A = Adjacency.from_graph(src, config.device)
+    B = Adjacency.from_graph(tgt, config.device)
+    torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        align(A, B, config, Profile())
+    torch.cuda.synchronize()
+    barrier(world)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    N.timing_reset()
+    N.timing_enable(True)
+    launches0 = N.launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    profiles = []
+    for _ in range(args.steps):
+        prof = Profile()
+        P, cols, count = align(A, B, config, prof)
+        profiles.append(prof)
+    stop.record()
+    torch.cuda.synchronize()
+    launches = N.launch_count() - launches0
+    N.timing_enable(False)
+    clk = clocks.stop()
+    elapsed = start.elapsed_time(stop) / 1000.0
+    elapsed = max_over_ranks(elapsed, world, dev)
+    fam = {name: N.timing_query(k) for k, name in enumerate(N.KERNEL_FAMILY_NAMES)}
+    cols_np = cols.cpu().numpy() if isinstance(cols, torch.Tensor) else np.asarray(cols)
+    accuracy = float(np.mean(cols_np == perm))
+    profiles[-1].resolve()
+    sk = [p.iteration_count for p in profiles[-1].sinkhorn_profiles]
+    mean_sweeps = float(np.mean(sk)) if sk else 0.0
+
+    # end-to-end through cugal() from host graphs
+    import networkx as nx
+    e2e_times = []
+    h2d = 0
+    for _ in range(args.e2e_steps):
+        s_copy, t_copy = nx.Graph(src), nx.Graph(tgt)
+        h2d = (edge_array(s_copy).nbytes + edge_array(t_copy).nbytes)
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        Ph, mapping = cugal(s_copy, t_copy, config, Profile())
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e = max_over_ranks(statistics.median(e2e_times), world, dev) if e2e_times else None
+    d2h = n * n * 4 + n * 8
+    e2e_acc = node_accuracy(mapping, perm) if e2e_times else None
+
+    ld = padded_ld(n)
+    peak, peak_kind = load_peak()
+    fam_key = "sweep16" if sdt is not None else "sweep32"
+    nl, ms = fam[fam_key]
+    elem = 2 if sdt is not None else 4
+    bytes_per = n * ld * elem
+    achieved = bytes_per / (ms / nl / 1e3) / 1e9 if nl else None
+    traffic = traffic_per_launch(n, ld) if sdt is not None else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        solves = config.iter_count * config.frank_wolfe_iter_count
+        v, cores, sample = cpu_alignment_seconds(n, solves, mean_sweeps or config.sinkhorn_iterations,
+                                                 args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        value = elapsed / args.steps
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1000.0, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"bf16": "bf16", "fp16": "f16", "fp32": "f32"}[args.stream_dtype],
+            "data": "synthetic",
+            "config": {"workload": w.name, "n": n, "edges_source": src.number_of_edges(),
+                       "edges_target": tgt.number_of_edges(), "stream_dtype": args.stream_dtype,
+                       "fw_steps": config.iter_count * config.frank_wolfe_iter_count,
+                       "sinkhorn_iterations": config.sinkhorn_iterations, "reg": config.sinkhorn_regularization,
+                       "lap": config.hungarian_method.value, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (cost copy n*ld*2 bytes)"},
+            "node_accuracy": accuracy, "e2e_node_accuracy": e2e_acc,
+            "mean_sinkhorn_iterations": mean_sweeps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": f"sweep_kernel<{args.stream_dtype}>", "launches": nl,
+                         "avg_launch_ms": ms / nl if nl else None, "bytes_per_launch": bytes_per,
+                         "peak_kind": peak_kind},
+            "kernel_times_ms": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in fam.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+// Shared device helpers for the FUGAL kernels (sm_100a).
+//
+// Everything here is generic: warp reductions, 16-byte vector loads of
+// fp32 / bf16 / fp16 rows into fp32 registers, mbarrier + bulk-copy wrappers
+// (inline PTX) used by the Sinkhorn sweep pipeline, and the bounded-wait
+// policy: every spin on an mbarrier gives up after a fixed number of polls,
+// records an error code in device memory and lets the kernel return.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fugal_b200.h"
+
+#define FUGAL_DEVICE __device__ __forceinline__
+
+namespace fugal {
+
+// A wait on an mbarrier gives up after kWaitLimitNs of %globaltimer time (or
+// kMaxPolls probes, whichever comes first); the kernel then records
+// FUGAL_DEVICE_TIMEOUT and returns instead of spinning forever.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+constexpr uint32_t kMaxPolls = 1u << 26;
+constexpr uint32_t kSuspendHintNs = 20000u;       // per try_wait
+
+FUGAL_DEVICE uint64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Device-side error word: the first failing wait writes its code here.
+FUGAL_DEVICE void report_error(int* flag, int code) {
+    if (flag != nullptr) atomicCAS(flag, 0, code);
+}
+
+// ---------------------------------------------------------------- reductions
+FUGAL_DEVICE float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+FUGAL_DEVICE float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+FUGAL_DEVICE double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide double sum (result valid in thread 0). `scratch` holds >= 32 doubles.
+FUGAL_DEVICE double block_sum(double v, double* scratch) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    const int nwarps = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nwarps) ? scratch[threadIdx.x] : 0.0;
+    if (warp == 0) v = warp_sum(v);
+    __syncthreads();
+    return v;
+}
+
+// Fast single-precision exp (CUDA's __expf intrinsic, the MUFU path; relative
+// error a few ulp, the same primitive the reference kernels use).
+FUGAL_DEVICE float fast_exp(float x) { return __expf(x); }
+
+// ------------------------------------------------------- element conversion
+template <typename T> struct Vec;  // one 16-byte chunk of T as fp32
+
+template <> struct Vec<float> {
+    static constexpr int N = 4;
+    FUGAL_DEVICE static void unpack(const uint4& r, float* out) {
+        out[0] = __uint_as_float(r.x); out[1] = __uint_as_float(r.y);
+        out[2] = __uint_as_float(r.z); out[3] = __uint_as_float(r.w);
+    }
+};
+template <> struct Vec<__nv_bfloat16> {
+    static constexpr int N = 8;
+    FUGAL_DEVICE static void unpack(const uint4& r, float* out) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            out[2 * i] = __uint_as_float(w[i] << 16);
+            out[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
+        }
+    }
+};
+template <> struct Vec<__half> {
+    static constexpr int N = 8;
+    FUGAL_DEVICE static void unpack(const uint4& r, float* out) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            __half2 h = *reinterpret_cast<const __half2*>(&w[i]);
+            float2 f = __half22float2(h);
+            out[2 * i] = f.x;
+            out[2 * i + 1] = f.y;
+        }
+    }
+};
+
+template <typename T> FUGAL_DEVICE T from_float(float x);
+template <> FUGAL_DEVICE float from_float<float>(float x) { return x; }
+template <> FUGAL_DEVICE __nv_bfloat16 from_float<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+template <> FUGAL_DEVICE __half from_float<__half>(float x) { return __float2half_rn(x); }
+
+// ------------------------------------------------------------ PTX wrappers
+FUGAL_DEVICE uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+FUGAL_DEVICE void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+FUGAL_DEVICE void fence_mbarrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+FUGAL_DEVICE void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+FUGAL_DEVICE void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// Non-blocking probe of phase `parity`; true once that phase has completed.
+FUGAL_DEVICE bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n"
+        " mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendHintNs)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: returns false (and records FUGAL_DEVICE_TIMEOUT) if the phase
+// does not complete within kWaitLimitNs.
+FUGAL_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_timer_ns();
+    for (uint32_t i = 0; i < kMaxPolls; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_timer_ns() - t0 > kWaitLimitNs) break;
+    }
+    report_error(err, FUGAL_DEVICE_TIMEOUT);
+    return false;
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, completing on `bar`.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+FUGAL_DEVICE void bulk_load(void* smem_dst, const void* gmem_src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(smem_dst)),
+        "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// ------------------------------------------------------------ cluster / DSMEM
+FUGAL_DEVICE uint32_t cluster_ctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+FUGAL_DEVICE uint32_t cluster_nctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+FUGAL_DEVICE uint32_t cluster_id_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+FUGAL_DEVICE uint32_t ncluster_x() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+FUGAL_DEVICE void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Address of the same shared variable in CTA `rank` of this cluster.
+FUGAL_DEVICE uint32_t map_to_rank(const void* p, uint32_t rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(smem_addr(p)), "r"(rank));
+    return out;
+}
+FUGAL_DEVICE void st_cluster_f32x2(uint32_t addr, float a, float b) {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(a), "f"(b) : "memory");
+}
+FUGAL_DEVICE void mbar_arrive_cluster(uint32_t remote_bar_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote_bar_addr)
+                 : "memory");
+}
+
+}  // namespace fugal

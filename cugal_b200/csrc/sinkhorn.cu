@@ -1,0 +1,1034 @@
+// Log-domain Sinkhorn for the FUGAL Frank-Wolfe step (cugal/sinkhorn.py:90-120).
+//
+// Reference semantics, per iteration t (0-based):
+//     v <- (1-w) v - w * LSE_i(K_ij + u_i)        column update
+//     u <- (1-w) u - w * LSE_j(K_ij + v_j)        row update
+//     if t % eval_freq == 0 and t != 0: err = sum_j |sum_i exp(K+u+v)_ij - 1|, stop if err < tol
+// The reference reads K four times per iteration (two passes per LSE, a
+// transposed copy for the columns) and syncs the host after every launch.
+//
+// Here one kernel ("sweep") does a whole iteration boundary in ONE read of the
+// cost: it computes the row update of iteration t and, while each row is still
+// in registers, adds the row-normalised plan P_ij = exp(K_ij + u_i + v_j) into
+// per-column sums.  Those sums are (a) exactly the column marginals the
+// reference's convergence check measures after iteration t and (b) all the
+// column update of iteration t+1 needs: v_j <- v_j - w log(colsum_j).  A small
+// "finalize" kernel reduces the per-cluster column sums in FP64, records the
+// error, takes the stop / momentum decision on the device and leaves
+// log(colsum) for the next sweep, which applies it to v when it loads it (so a
+// momentum change at an evaluation point affects v_{t+1} as in the reference).
+// Only the first column update of a solve is a separate max-stabilised pass.
+//
+// Row layout: each cluster of C CTAs owns a contiguous block of rows; CTA k of
+// the cluster owns column slice k.  Row slices stream HBM -> shared memory with
+// 1-D bulk copies (cp.async.bulk + mbarrier, several stages in flight); the
+// per-row (max, sum) partials of the C CTAs are exchanged through distributed
+// shared memory (remote stores + remote mbarrier arrives, double-buffered).
+// Every thread keeps its 16 columns' running column sums in registers for the
+// whole sweep, so the only global writes are one partial row per cluster.
+//
+// Precision: the cost arrives "absorbed" (cost32 = K + U_i + V_j with the
+// previous solves' duals U, V folded in), so its entries are ~log P and the
+// duals handled here are small increments.  With a BF16/FP16 stream the solve
+// reads cost32 for the first sweeps, then an "absorb" sweep writes the reduced-
+// precision copy cost16 = cost32 + a_i + b_j (~ log P after the row update,
+// rounded once), re-absorbed from cost32 every reabsorb_every sweeps, and ends
+// with FP32 polish sweeps on cost32.  LSE, duals and sums are FP32; the
+// convergence reduction and the step decisions are FP64.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+#include "fugal_common.cuh"
+#include "fugal_host.h"
+
+namespace fugal {
+
+constexpr int kMaxStages = 8;
+constexpr int kMaxCluster = 16;
+constexpr int kKPT = 16;  // columns per thread
+
+struct SolveState {
+    int it;          // index of the next sweep
+    int done;        // set when the current phase has finished
+    int final_it;    // index of the last sweep of the current phase
+    int n_err;
+    unsigned int ticket;
+    int status;      // device-side error code (bounded waits)
+    int max_it;      // phase ends after sweep max_it - 1
+    int check;       // 1: main phase (convergence checks), 0: polish
+    int eval_freq;
+    int momentum_start;
+    int main_final_it;
+    int main_n_err;
+    int polish_count;
+    int pad0;
+    double threshold;
+    double omega;
+    double err_accum;
+    double last_err;
+    double main_last_err;
+    double polish_err;
+    double errors[FUGAL_MAX_RECORDED_ERRORS];
+};
+
+// ------------------------------------------------------------------ device
+
+// SinkhornState.lehmann_momentum (cugal/sinkhorn.py:78-88) with Python list
+// indexing (negative indices count from the end).
+__device__ double lehmann_momentum(const SolveState* st) {
+    const int len = st->n_err;
+    if (st->momentum_start < 0 || (long long)len * st->eval_freq < st->momentum_start) return 1.0;
+    const int index = st->momentum_start / st->eval_freq;
+    if (len < index - 1) return 1.0;
+    int i1 = index - 1, i2 = index - 2;
+    if (i1 < 0) i1 += len;
+    if (i2 < 0) i2 += len;
+    if (i1 < 0 || i2 < 0 || i1 >= len || i2 >= len || i1 >= FUGAL_MAX_RECORDED_ERRORS ||
+        i2 >= FUGAL_MAX_RECORDED_ERRORS)
+        return 1.0;
+    double ratio = st->errors[i1] / st->errors[i2];
+    if (isnan(ratio)) ratio = 0.99;
+    ratio = fmin(ratio, 0.99);
+    const double power = 1.0 / st->eval_freq;
+    return 2.0 / (1.0 + sqrt(1.0 - pow(ratio, power)));
+}
+
+// End-of-sweep decision (single thread).
+__device__ void decide(SolveState* st, double err) {
+    const int t = st->it;
+    st->last_err = err;
+    bool stop = false;
+    if (st->check) {
+        if (t % st->eval_freq == 0 && t != 0) {
+            if (st->n_err < FUGAL_MAX_RECORDED_ERRORS) st->errors[st->n_err] = err;
+            st->n_err += 1;
+            if (err < st->threshold)
+                stop = true;
+            else
+                st->omega = lehmann_momentum(st);
+        }
+    } else {
+        st->polish_err = err;
+        st->polish_count += 1;
+    }
+    if (!stop && t + 1 >= st->max_it) stop = true;
+    if (stop) {
+        st->done = 1;
+        st->final_it = t;
+        if (st->check) {
+            st->main_final_it = t;
+            st->main_n_err = st->n_err;
+            st->main_last_err = err;
+        }
+    }
+    st->it = t + 1;
+}
+
+struct SweepArgs {
+    const void* L;        // cost (element type T), n x ld
+    long long ld;
+    int n;
+    int n_copy;           // columns copied per row (multiple of 16 bytes)
+    int slice_w;          // columns per CTA = THREADS * kKPT
+    int rows_per_cluster;
+    int stages;
+    const float* b_buf;   // [2][n_pad] column duals of consecutive sweeps
+    const float* b_off;   // frame offset added to the previous b (nullable)
+    const float* logcs;   // log column sums of the previous sweep
+    float* b_buf_w;       // same as b_buf (written slot)
+    float* a;             // row duals (read for momentum, written)
+    const float* a_off;   // frame offset added to the previous a (nullable)
+    float* partials;      // [clusters][n_pad]
+    long long n_pad;
+    SolveState* st;
+    void* out16;          // ABSORB: reduced-precision copy written here
+    long long ld16;
+    float* a_snap;        // ABSORB: absorbed row duals
+    float* b_snap;        // ABSORB: absorbed column duals
+};
+
+constexpr int kBarBytes = 128;
+
+template <int THREADS, int R>
+__host__ __device__ constexpr int header_bytes() {
+    // barriers + red_max/red_sum [WARPS][R] + xch [2][kMaxCluster][R] float2, rounded to 128
+    return ((kBarBytes + 2 * (THREADS / 32) * R * 4 + 2 * kMaxCluster * R * 8) + 127) / 128 * 128;
+}
+
+template <typename T, int THREADS, int R, bool ABSORB, typename TOUT>
+__global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
+    constexpr int V = Vec<T>::N;
+    constexpr int G = kKPT / V;
+    constexpr int WARPS = THREADS / 32;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* xbar = full + kMaxStages;
+    float* red_max = reinterpret_cast<float*>(smem + kBarBytes);
+    float* red_sum = red_max + WARPS * R;
+    float2* xch = reinterpret_cast<float2*>(red_sum + WARPS * R);
+    float* b_s = reinterpret_cast<float*>(smem + header_bytes<THREADS, R>());
+    unsigned char* stage_base = reinterpret_cast<unsigned char*>(b_s + p.slice_w);
+
+    SolveState* st = p.st;
+    if (*reinterpret_cast<volatile int*>(&st->done)) return;  // uniform: written by an earlier kernel
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int C = (int)cluster_nctarank();
+    const int rank = (int)cluster_ctarank();
+    const int cid = (int)cluster_id_x();
+    const int n = p.n;
+    const int col0 = rank * p.slice_w;
+    const int ncopy = max(0, min(p.slice_w, p.n_copy - col0));
+    const int nvalid = max(0, min(p.slice_w, n - col0));
+    const int row_begin = cid * p.rows_per_cluster;
+    const int row_end = min(n, row_begin + p.rows_per_cluster);
+    const int nbatch = row_end > row_begin ? (row_end - row_begin + R - 1) / R : 0;
+    const int t = st->it;
+    const float omega = static_cast<float>(st->omega);
+    const bool momentum = fabsf(omega - 1.0f) > 0.0f;
+    const uint32_t row_bytes = static_cast<uint32_t>(ncopy) * sizeof(T);
+    const size_t stage_bytes = static_cast<size_t>(R) * p.slice_w * sizeof(T);
+    const float* b_prev = p.b_buf + ((t - 1) & 1) * p.n_pad;
+    float* b_out = p.b_buf_w + (t & 1) * p.n_pad;
+
+    // Column duals of this sweep: b = b_off + b_prev - w log(colsum_prev).
+    for (int j = tid; j < p.slice_w; j += THREADS) {
+        float b = 0.f;
+        if (j < nvalid) {
+            const int jg = col0 + j;
+            b = b_prev[jg] - omega * p.logcs[jg];
+            if (p.b_off != nullptr) b += p.b_off[jg];
+            if (cid == 0) {
+                if (ABSORB) {
+                    p.b_snap[jg] = b;
+                    b_out[jg] = 0.f;
+                } else {
+                    b_out[jg] = b;
+                }
+            }
+        }
+        b_s[j] = b;
+    }
+    if (tid == 0) {
+        for (int s = 0; s < p.stages; ++s) mbar_init(&full[s], 1);
+        mbar_init(&xbar[0], C);
+        mbar_init(&xbar[1], C);
+        fence_mbarrier_init();
+    }
+    __syncthreads();
+    if (C > 1) cluster_sync();  // every peer's barriers exist before the first remote arrive
+
+    auto issue = [&](int bt) {
+        const int s = bt % p.stages;
+        const int r0 = row_begin + bt * R;
+        const int rows = min(R, row_end - r0);
+        unsigned char* dst = stage_base + s * stage_bytes;
+        mbar_arrive_expect_tx(&full[s], rows * row_bytes);
+        if (row_bytes > 0) {
+            const T* src = static_cast<const T*>(p.L) + static_cast<size_t>(r0) * p.ld + col0;
+            for (int r = 0; r < rows; ++r)
+                bulk_load(dst + static_cast<size_t>(r) * p.slice_w * sizeof(T), src + static_cast<size_t>(r) * p.ld,
+                          row_bytes, &full[s]);
+        }
+    };
+    int issued = 0;
+    if (tid == 0) {
+        issued = min(p.stages, nbatch);
+        for (int bt = 0; bt < issued; ++bt) issue(bt);
+    }
+
+    float acc[kKPT];
+#pragma unroll
+    for (int k = 0; k < kKPT; ++k) acc[k] = 0.f;
+
+    int bt = 0;
+    for (; bt < nbatch; ++bt) {
+        const int s = bt % p.stages;
+        const bool okw = mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status);
+        const int r0 = row_begin + bt * R;
+        const int rows = min(R, row_end - r0);
+        const T* stage = reinterpret_cast<const T*>(stage_base + s * stage_bytes);
+
+        float e[R][kKPT];
+        float mx[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) mx[r] = -INFINITY;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int c = (g * THREADS + tid) * V;
+            float bv[V];
+#pragma unroll
+            for (int q = 0; q < V; q += 4) {
+                const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + q);
+                bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (r < rows) {
+                    const uint4 raw = *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
+                    float vals[V];
+                    Vec<T>::unpack(raw, vals);
+#pragma unroll
+                    for (int q = 0; q < V; ++q) {
+                        const float x = (c + q < nvalid) ? vals[q] + bv[q] : -INFINITY;
+                        e[r][g * V + q] = x;
+                        mx[r] = fmaxf(mx[r], x);
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < V; ++q) e[r][g * V + q] = -INFINITY;
+                }
+            }
+        }
+        float a_old[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            a_old[r] = 0.f;
+            if (momentum && r < rows) {
+                a_old[r] = p.a[r0 + r];
+                if (p.a_off != nullptr) a_old[r] += p.a_off[r0 + r];
+            }
+            mx[r] = warp_max(mx[r]);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) red_max[warp * R + r] = mx[r];
+        }
+        if (!__syncthreads_and(okw)) break;  // S1: stage s fully read into registers
+        if (!ABSORB && tid == 0 && bt + p.stages < nbatch) {
+            fence_proxy_async_smem();
+            issue(bt + p.stages);
+            ++issued;
+        }
+        float Mc[R], sm[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float m = -INFINITY;
+#pragma unroll
+            for (int w = 0; w < WARPS; ++w) m = fmaxf(m, red_max[w * R + r]);
+            Mc[r] = m;
+            const float base = (m == -INFINITY) ? 0.f : m;
+            float ssum = 0.f;
+#pragma unroll
+            for (int k = 0; k < kKPT; ++k) {
+                const float y = fast_exp(e[r][k] - base);
+                e[r][k] = y;
+                ssum += y;
+            }
+            sm[r] = warp_sum(ssum);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) red_sum[warp * R + r] = sm[r];
+        }
+        __syncthreads();  // S2
+        float M[R], S[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float ssum = 0.f;
+#pragma unroll
+            for (int w = 0; w < WARPS; ++w) ssum += red_sum[w * R + r];
+            M[r] = Mc[r];
+            S[r] = ssum;
+        }
+        if (C > 1) {
+            const int slot = bt & 1;
+            bool okx = true;
+            if (tid == 0) {
+                for (int k = 0; k < C; ++k) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        st_cluster_f32x2(map_to_rank(&xch[(slot * kMaxCluster + rank) * R + r], k), Mc[r], S[r]);
+                    mbar_arrive_cluster(map_to_rank(&xbar[slot], k));
+                }
+                okx = mbar_wait(&xbar[slot], static_cast<uint32_t>((bt >> 1) & 1), &st->status);
+            }
+            if (!__syncthreads_and(okx)) break;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                float m = -INFINITY;
+                for (int k = 0; k < C; ++k) m = fmaxf(m, xch[(slot * kMaxCluster + k) * R + r].x);
+                float ssum = 0.f;
+                for (int k = 0; k < C; ++k) {
+                    const float2 ps = xch[(slot * kMaxCluster + k) * R + r];
+                    if (ps.x != -INFINITY) ssum += ps.y * fast_exp(ps.x - m);
+                }
+                M[r] = m;
+                S[r] = ssum;
+            }
+        }
+        // Row update and the scale that turns e into the plan: P_ij = e_ij * w_r.
+        float anew[R], wr[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float lse = M[r] + logf(S[r]);
+            anew[r] = momentum ? (1.f - omega) * a_old[r] - omega * lse : -lse;
+            wr[r] = (Mc[r] == -INFINITY) ? 0.f : fast_exp(Mc[r] + anew[r]);
+        }
+        if (rank == 0 && tid < rows) {
+            float v = anew[0];
+#pragma unroll
+            for (int r = 1; r < R; ++r)
+                if (tid == r) v = anew[r];
+            if (ABSORB) {
+                p.a_snap[r0 + tid] = v;
+                p.a[r0 + tid] = 0.f;
+            } else {
+                p.a[r0 + tid] = v;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r < rows) {
+#pragma unroll
+                for (int k = 0; k < kKPT; ++k) acc[k] = fmaf(e[r][k], wr[r], acc[k]);
+            }
+        }
+        if (ABSORB) {
+            // cost16 = cost32 + b_j + a_i  (~ log P after this row update), rounded once
+            constexpr int VO = V;  // T is float here: 4 outputs per chunk
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int c = (g * THREADS + tid) * V;
+                if (c < ncopy) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        if (r < rows) {
+                            const uint4 raw =
+                                *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
+                            float vals[V];
+                            Vec<T>::unpack(raw, vals);
+                            TOUT o[VO];
+#pragma unroll
+                            for (int q = 0; q < VO; ++q)
+                                o[q] = from_float<TOUT>((c + q < nvalid) ? vals[q] + b_s[c + q] + anew[r]
+                                                                         : -INFINITY);
+                            TOUT* dst = static_cast<TOUT*>(p.out16) + static_cast<size_t>(r0 + r) * p.ld16 + col0 + c;
+                            *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(o);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid == 0 && bt + p.stages < nbatch) {
+                fence_proxy_async_smem();
+                issue(bt + p.stages);
+                ++issued;
+            }
+        }
+    }
+
+    // Per-cluster column sums of the row-normalised plan.
+    float* prow = p.partials + static_cast<size_t>(cid) * p.n_pad + col0;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int c = (g * THREADS + tid) * V;
+#pragma unroll
+        for (int q = 0; q < V; ++q)
+            if (c + q < nvalid) prow[c + q] = acc[g * V + q];
+    }
+
+    // An early exit (timed-out wait) may leave bulk copies in flight: wait for
+    // them, again bounded, before the shared memory goes away.
+    if (bt < nbatch && tid == 0) {
+        for (int b = bt; b < issued; ++b)
+            if (!mbar_wait(&full[b % p.stages], static_cast<uint32_t>((b / p.stages) & 1), &st->status)) break;
+    }
+    if (C > 1) cluster_sync();  // no CTA leaves while a peer may still write its shared memory
+}
+
+// Reduce the per-cluster column sums (FP64), write log(colsum), decide.
+__global__ void finalize_kernel(const float* partials, int nparts, long long n_pad, int n, float* logcs,
+                                SolveState* st) {
+    __shared__ double red[32];
+    if (*reinterpret_cast<volatile int*>(&st->done)) return;
+    double err = 0.0;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        double cs = 0.0;
+        for (int c = 0; c < nparts; ++c) cs += static_cast<double>(partials[static_cast<size_t>(c) * n_pad + j]);
+        err += fabs(cs - 1.0);
+        logcs[j] = static_cast<float>(log(fmax(cs, 1e-37)));
+    }
+    err = block_sum(err, red);
+    if (threadIdx.x == 0) {
+        atomicAdd(&st->err_accum, err);
+        __threadfence();
+        const unsigned prev = atomicAdd(&st->ticket, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            const double total = atomicAdd(&st->err_accum, 0.0);
+            st->err_accum = 0.0;
+            st->ticket = 0;
+            decide(st, total);
+        }
+    }
+}
+
+// First column update of a solve, max-stabilised: per (row chunk, column) an
+// online (max, sum) of exp(cost_ij + a_i).
+__global__ void __launch_bounds__(256) column_pass_kernel(const float* L, long long ld, int n, const float* a,
+                                                          int rows_per_chunk, float2* part, long long n_pad) {
+    const int j0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int chunk = blockIdx.y;
+    const int i0 = chunk * rows_per_chunk;
+    const int i1 = min(n, i0 + rows_per_chunk);
+    if (j0 >= n) return;
+    const bool full4 = (j0 + 4 <= n) && ((ld & 3) == 0);
+    float m[4], s[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        m[q] = -INFINITY;
+        s[q] = 0.f;
+    }
+    for (int i = i0; i < i1; i += 4) {
+        float x[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int row = i + r;
+            if (row < i1) {
+                const float ai = a[row];
+                const float* src = L + static_cast<size_t>(row) * ld + j0;
+                if (full4) {
+                    const float4 v = *reinterpret_cast<const float4*>(src);
+                    x[r][0] = v.x + ai; x[r][1] = v.y + ai; x[r][2] = v.z + ai; x[r][3] = v.w + ai;
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) x[r][q] = (j0 + q < n) ? src[q] + ai : -INFINITY;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) x[r][q] = -INFINITY;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float mn = fmaxf(fmaxf(m[q], fmaxf(x[0][q], x[1][q])), fmaxf(x[2][q], x[3][q]));
+            if (mn == -INFINITY) continue;
+            float acc = (m[q] == -INFINITY) ? 0.f : s[q] * expf(m[q] - mn);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc += expf(x[r][q] - mn);
+            m[q] = mn;
+            s[q] = acc;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (j0 + q < n) part[static_cast<size_t>(chunk) * n_pad + j0 + q] = make_float2(m[q], s[q]);
+}
+
+struct InitArgs {
+    int max_it;
+    int eval_freq;
+    int momentum_start;
+    double threshold;
+};
+
+// Merge the column-pass partials into v_0 = -LSE_i(cost + a) (momentum is 1 at
+// iteration 0), stored as the "previous sweep" b, with a zero pending
+// correction; block 0 also resets the solve state.
+__global__ void column_merge_kernel(const float2* part, int nchunks, long long n_pad, int n, float* b_buf,
+                                    float* logcs, SolveState* st, InitArgs ia) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->it = 0;
+        st->done = 0;
+        st->final_it = -1;
+        st->n_err = 0;
+        st->ticket = 0;
+        st->status = 0;
+        st->max_it = ia.max_it;
+        st->check = 1;
+        st->eval_freq = ia.eval_freq;
+        st->momentum_start = ia.momentum_start;
+        st->main_final_it = -1;
+        st->main_n_err = 0;
+        st->polish_count = 0;
+        st->threshold = ia.threshold;
+        st->omega = 1.0;
+        st->err_accum = 0.0;
+        st->last_err = 0.0;
+        st->main_last_err = 0.0;
+        st->polish_err = 0.0;
+    }
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        float M = -INFINITY;
+        for (int c = 0; c < nchunks; ++c) M = fmaxf(M, part[static_cast<size_t>(c) * n_pad + j].x);
+        float S = 0.f;
+        if (M != -INFINITY)
+            for (int c = 0; c < nchunks; ++c) {
+                const float2 ps = part[static_cast<size_t>(c) * n_pad + j];
+                if (ps.x != -INFINITY) S += ps.y * expf(ps.x - M);
+            }
+        b_buf[n_pad + j] = -(M + logf(S));  // slot of sweep -1
+        logcs[j] = 0.f;
+    }
+}
+
+struct FrameArgs {
+    int stream16;      // 1 if a reduced-precision phase exists
+    int warmup;        // first reduced-precision sweep index (the absorb sweep)
+    int every;         // reabsorb period
+    int polish;        // polish sweeps requested
+};
+
+// Index of the snapshot that defines the frame of sweep t (or -1 for FP32).
+__device__ int frame_snapshot(const FrameArgs& f, int t) {
+    if (!f.stream16 || t < f.warmup) return -1;
+    return ((t - f.warmup) / f.every) & 1;
+}
+
+// Move the final main-phase duals into the FP32 frame and open the polish phase.
+__global__ void polish_begin_kernel(SolveState* st, float* a, float* b_buf, long long n_pad, float* logcs,
+                                    const float* a_snap, const float* b_snap, int n, FrameArgs f) {
+    const int fin = st->final_it;
+    const int snap = frame_snapshot(f, fin);
+    float* b = b_buf + (fin & 1) * n_pad;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        if (snap >= 0) {
+            b[j] += b_snap[snap * n_pad + j];
+            a[j] += a_snap[snap * n_pad + j];
+        }
+        logcs[j] = 0.f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->done = 0;
+        st->it = fin + 1;
+        st->max_it = fin + 1 + f.polish;
+        st->check = 0;
+        st->omega = 1.0;
+    }
+}
+
+// Final duals (FP32 frame) and the record.
+__global__ void solve_end_kernel(const SolveState* st, const float* a, const float* b_buf, long long n_pad,
+                                 const float* a_snap, const float* b_snap, int n, FrameArgs f, float* u_out,
+                                 float* v_out, fugal_solve_record* rec) {
+    const int fin = st->final_it;
+    const bool polished = st->check == 0;
+    const int snap = polished ? -1 : frame_snapshot(f, fin);
+    const float* b = b_buf + (fin & 1) * n_pad;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        u_out[j] = a[j] + (snap >= 0 ? a_snap[snap * n_pad + j] : 0.f);
+        v_out[j] = b[j] + (snap >= 0 ? b_snap[snap * n_pad + j] : 0.f);
+    }
+    if (rec != nullptr && blockIdx.x == 0) {
+        for (int k = threadIdx.x; k < FUGAL_MAX_RECORDED_ERRORS; k += blockDim.x) rec->errors[k] = st->errors[k];
+        if (threadIdx.x == 0) {
+            rec->iteration_count = st->main_final_it + 1;
+            rec->n_errors = min(st->main_n_err, FUGAL_MAX_RECORDED_ERRORS);
+            rec->status = st->status;
+            rec->polish_count = st->polish_count;
+            rec->last_error = st->main_last_err;
+            rec->polish_error = st->polish_err;
+        }
+    }
+}
+
+// ------------------------------------------------------------------- host
+
+namespace {
+
+struct SweepPlan {
+    int threads;
+    int R;
+    int cluster;
+    int slice_w;
+    int clusters;       // number of clusters in the grid
+    int rows_per_cluster;
+    int stages;
+    size_t smem;
+};
+
+int elem_size(int dt) { return dt == FUGAL_F32 ? 4 : 2; }
+
+using KernelFn = void (*)(const SweepArgs);
+
+// Rows per batch: 4 for 16-bit streams up to 256 threads, else 2 (keeps the
+// 16 x R exponentials of a thread in registers without spilling at 512 threads).
+constexpr int rows_per_batch(int elem_bytes, int threads) { return (elem_bytes == 4 || threads == 512) ? 2 : 4; }
+
+template <typename T, int THREADS, bool ABSORB, typename TOUT>
+KernelFn pick_kernel() {
+    constexpr int R = rows_per_batch(sizeof(T), THREADS);
+    return sweep_kernel<T, THREADS, R, ABSORB, TOUT>;
+}
+
+// kind: 0 = plain sweep over dtype dt, 1 = absorb (fp32 -> bf16), 2 = absorb (fp32 -> fp16)
+template <int THREADS>
+KernelFn kernel_for(int dt, int kind) {
+    if (kind == 1) return pick_kernel<float, THREADS, true, __nv_bfloat16>();
+    if (kind == 2) return pick_kernel<float, THREADS, true, __half>();
+    if (dt == FUGAL_BF16) return pick_kernel<__nv_bfloat16, THREADS, false, float>();
+    if (dt == FUGAL_F16) return pick_kernel<__half, THREADS, false, float>();
+    return pick_kernel<float, THREADS, false, float>();
+}
+
+KernelFn kernel_for(int threads, int dt, int kind) {
+    if (threads == 128) return kernel_for<128>(dt, kind);
+    if (threads == 256) return kernel_for<256>(dt, kind);
+    return kernel_for<512>(dt, kind);
+}
+
+int header_for(int threads, int R) {
+    if (threads == 128) return R == 2 ? header_bytes<128, 2>() : header_bytes<128, 4>();
+    if (threads == 256) return R == 2 ? header_bytes<256, 2>() : header_bytes<256, 4>();
+    return R == 2 ? header_bytes<512, 2>() : header_bytes<512, 4>();
+}
+
+int max_smem_optin() {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0)
+        v = 227 * 1024;
+    return v;
+}
+
+// Largest column slice per CTA (THREADS * 16): 8192 by default; the
+// environment variable FUGAL_SWEEP_SLICE (2048, 4096 or 8192) lowers it, which
+// trades larger clusters for fewer threads per CTA.
+int max_slice() {
+    const char* e = getenv("FUGAL_SWEEP_SLICE");
+    const int v = e ? atoi(e) : 8192;
+    return (v == 2048 || v == 4096) ? v : 8192;
+}
+
+// Launch shape for n columns: threads per CTA and CTAs per cluster, so that
+// cluster * threads * 16 >= n with the smallest cluster.
+fugal_status plan_shape(int64_t n, int& threads, int& cluster) {
+    if (n <= 2048) { threads = 128; cluster = 1; return FUGAL_OK; }
+    if (n <= 4096 && max_slice() >= 4096) { threads = 256; cluster = 1; return FUGAL_OK; }
+    const int slice = max_slice();
+    threads = slice / kKPT;
+    cluster = 1;
+    while (static_cast<int64_t>(cluster) * slice < n) cluster <<= 1;
+    if (cluster > kMaxCluster)
+        return fail(FUGAL_BAD_SHAPE, "sinkhorn: n = %lld exceeds the supported maximum %d", (long long)n,
+                    kMaxCluster * slice);
+    return FUGAL_OK;
+}
+
+fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_occupancy) {
+    FUGAL_TRY(plan_shape(n, pl.threads, pl.cluster));
+    const int es = (kind != 0) ? 4 : elem_size(dt);
+    pl.R = rows_per_batch(es, pl.threads);
+    pl.slice_w = pl.threads * kKPT;
+    const size_t stage_bytes = static_cast<size_t>(pl.R) * pl.slice_w * es;
+    const size_t fixed = header_for(pl.threads, pl.R) + static_cast<size_t>(pl.slice_w) * 4;
+    const int budget = max_smem_optin();
+    int stages = static_cast<int>((budget - static_cast<int64_t>(fixed)) / static_cast<int64_t>(stage_bytes));
+    stages = std::min(stages, kMaxStages);
+    if (pl.threads < 512) stages = std::min(stages, 4);  // small slices: leave room for 2+ CTAs per SM
+    if (stages < 1) return fail(FUGAL_BAD_SHAPE, "sinkhorn: no shared-memory stage fits");
+    pl.stages = stages;
+    pl.smem = fixed + stages * stage_bytes;
+    const int sms = sm_count();
+    int clusters = sms / pl.cluster;
+    if (query_occupancy) {
+        KernelFn fn = kernel_for(pl.threads, dt, kind);
+        FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem),
+                             "sinkhorn: set dynamic shared memory"));
+        if (pl.cluster > 8)
+            FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+                                 "sinkhorn: allow cluster size 16"));
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim = dim3(pl.cluster, 1, 1);
+        cfg.blockDim = dim3(pl.threads, 1, 1);
+        cfg.dynamicSmemBytes = pl.smem;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = pl.cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int active = 0;
+        FUGAL_TRY(cuda_check(cudaOccupancyMaxActiveClusters(&active, fn, &cfg), "sinkhorn: occupancy query"));
+        if (active <= 0) return fail(FUGAL_UNSUPPORTED, "sinkhorn: cluster of %d CTAs cannot be scheduled", pl.cluster);
+        clusters = active;
+    } else {
+        clusters = sms * 4;  // upper bound for workspace sizing
+    }
+    const int max_useful = static_cast<int>((n + pl.R - 1) / pl.R);
+    clusters = std::max(1, std::min(clusters, max_useful));
+    pl.clusters = clusters;
+    pl.rows_per_cluster = static_cast<int>((n + clusters - 1) / clusters);
+    return FUGAL_OK;
+}
+
+constexpr int kColThreads = 256;
+
+int colpass_chunks(int64_t n) {
+    const int col_blocks = static_cast<int>((n + kColThreads * 4 - 1) / (kColThreads * 4));
+    int chunks = std::max(1, (sm_count() * 8) / std::max(1, col_blocks));
+    chunks = std::min<int64_t>(chunks, std::max<int64_t>(1, n / 16));
+    return chunks;
+}
+
+struct Workspace {
+    SolveState* st;
+    float* b_buf;     // [2][n_pad]
+    float* logcs;     // [n_pad]
+    float* a;         // [n_pad]
+    float* a_snap;    // [2][n_pad]
+    float* b_snap;    // [2][n_pad]
+    float* partials;  // [max(sweep clusters, 2*column chunks)][n_pad]
+    long long n_pad;
+    size_t bytes;
+};
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+Workspace layout(int64_t n, char* base, int partial_rows) {
+    Workspace w{};
+    w.n_pad = static_cast<long long>(align_up(static_cast<size_t>(n), 64));
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char* p = base ? base + off : nullptr;
+        off = align_up(off + bytes, 256);
+        return p;
+    };
+    w.st = reinterpret_cast<SolveState*>(take(sizeof(SolveState)));
+    w.b_buf = reinterpret_cast<float*>(take(2 * w.n_pad * 4));
+    w.logcs = reinterpret_cast<float*>(take(w.n_pad * 4));
+    w.a = reinterpret_cast<float*>(take(w.n_pad * 4));
+    w.a_snap = reinterpret_cast<float*>(take(2 * w.n_pad * 4));
+    w.b_snap = reinterpret_cast<float*>(take(2 * w.n_pad * 4));
+    w.partials = reinterpret_cast<float*>(take(static_cast<size_t>(partial_rows) * w.n_pad * 4));
+    w.bytes = off;
+    return w;
+}
+
+int partial_rows_bound(int64_t n) {
+    return std::max(sm_count() * 4, 2 * colpass_chunks(n));
+}
+
+fugal_status launch_sweep(const SweepPlan& pl, KernelFn fn, const SweepArgs& args, cudaStream_t stream,
+                          int family) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(pl.clusters * pl.cluster, 1, 1);
+    cfg.blockDim = dim3(pl.threads, 1, 1);
+    cfg.dynamicSmemBytes = pl.smem;
+    cfg.stream = stream;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = pl.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    LaunchScope scope(family, stream);
+    return cuda_check(cudaLaunchKernelEx(&cfg, fn, args), "sinkhorn: sweep launch");
+}
+
+// Ring of pinned host words receiving the device "done" flag at each poll;
+// every solve takes two fresh slots so a late copy of an earlier solve on
+// another stream cannot be mistaken for this one's.
+constexpr int kPinnedSlots = 64;
+thread_local int* g_pinned_ring = nullptr;
+thread_local int g_pinned_next = 0;
+
+}  // namespace
+
+}  // namespace fugal
+
+using namespace fugal;
+
+extern "C" fugal_status fugal_sinkhorn_workspace_size(int64_t n, int stream_dtype, size_t* bytes) {
+    if (bytes == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_workspace_size: null output");
+    if (n <= 0) return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_workspace_size: n must be positive");
+    if (stream_dtype < FUGAL_F32 || stream_dtype > FUGAL_F16)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_workspace_size: bad stream dtype");
+    int threads, cluster;
+    FUGAL_TRY(plan_shape(n, threads, cluster));
+    *bytes = layout(n, nullptr, partial_rows_bound(n)).bytes;
+    return FUGAL_OK;
+}
+
+extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void* workspace, size_t workspace_bytes,
+                                             fugal_stream_t stream_) {
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    if (prm == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: null params");
+    const fugal_solve_params& p = *prm;
+    const int64_t n = p.n;
+    if (n <= 0) return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_solve: n must be positive");
+    if (p.cost32 == nullptr || p.u_out == nullptr || p.v_out == nullptr || workspace == nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: null pointer argument");
+    if (p.stream_dtype < FUGAL_F32 || p.stream_dtype > FUGAL_F16)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: bad stream dtype");
+    const bool use16 = p.stream_dtype != FUGAL_F32;
+    if (use16 && p.cost16 == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: cost16 is null");
+    if (p.max_iterations <= 0 || p.eval_freq <= 0)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: max_iterations and eval_freq must be positive");
+    if (p.ld32 < n || (p.ld32 % 4) != 0 || !aligned16(p.cost32))
+        return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_solve: cost32 needs ld >= n, ld %% 4 == 0, 16-byte base");
+    if (use16 && (p.ld16 < n || (p.ld16 % 8) != 0 || !aligned16(p.cost16)))
+        return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_solve: cost16 needs ld >= n, ld %% 8 == 0, 16-byte base");
+    if (use16 && (p.fp32_warmup_sweeps < 0 || p.reabsorb_every <= 0 || p.polish_sweeps < 0))
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: bad reduced-precision schedule");
+
+    const int prow = partial_rows_bound(n);
+    Workspace w = layout(n, static_cast<char*>(workspace), prow);
+    if (workspace_bytes < w.bytes)
+        return fail(FUGAL_WORKSPACE_TOO_SMALL, "fugal_sinkhorn_solve: workspace %zu < %zu bytes", workspace_bytes,
+                    w.bytes);
+
+    SweepPlan plan32, plan16, plan_abs;
+    FUGAL_TRY(make_plan(n, FUGAL_F32, 0, plan32, true));
+    if (use16) {
+        FUGAL_TRY(make_plan(n, p.stream_dtype, 0, plan16, true));
+        FUGAL_TRY(make_plan(n, FUGAL_F32, p.stream_dtype == FUGAL_BF16 ? 1 : 2, plan_abs, true));
+    }
+    if (plan32.clusters > prow || (use16 && (plan16.clusters > prow || plan_abs.clusters > prow)))
+        return fail(FUGAL_UNSUPPORTED, "fugal_sinkhorn_solve: more clusters than partial rows");
+
+    FrameArgs frame{use16 ? 1 : 0, use16 ? p.fp32_warmup_sweeps : 0, use16 ? p.reabsorb_every : 1,
+                    use16 ? p.polish_sweeps : 0};
+
+    // ---- iteration 0, column update: v_0 = -LSE_i(cost32_ij + a_i), a = 0
+    FUGAL_TRY(cuda_check(cudaMemsetAsync(w.a, 0, w.n_pad * 4, stream), "sinkhorn: clear row duals"));
+    const int chunks = colpass_chunks(n);
+    {
+        const int rows_per_chunk = static_cast<int>((n + chunks - 1) / chunks);
+        dim3 grid(static_cast<unsigned>((n + kColThreads * 4 - 1) / (kColThreads * 4)), chunks);
+        LaunchScope scope(FUGAL_KERNEL_COLUMN_PASS, stream);
+        column_pass_kernel<<<grid, kColThreads, 0, stream>>>(p.cost32, p.ld32, static_cast<int>(n), w.a,
+                                                              rows_per_chunk, reinterpret_cast<float2*>(w.partials),
+                                                              w.n_pad);
+        FUGAL_TRY(launch_check("sinkhorn: column pass"));
+    }
+    const int fin_blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 4 * sm_count()));
+    {
+        InitArgs ia{p.max_iterations, p.eval_freq, p.momentum_start < 0 ? -1 : p.momentum_start, p.threshold};
+        LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
+        column_merge_kernel<<<fin_blocks, 256, 0, stream>>>(reinterpret_cast<const float2*>(w.partials), chunks,
+                                                           w.n_pad, static_cast<int>(n), w.b_buf, w.logcs, w.st,
+                                                           ia);
+        FUGAL_TRY(launch_check("sinkhorn: column merge"));
+    }
+
+    auto sweep_args = [&](const SweepPlan& pl, const void* L, long long ld, const float* b_off,
+                          const float* a_off) {
+        SweepArgs a{};
+        a.L = L;
+        a.ld = ld;
+        a.n = static_cast<int>(n);
+        const int es = (L == p.cost32) ? 4 : elem_size(p.stream_dtype);
+        const int V = 16 / es;
+        a.n_copy = static_cast<int>((n + V - 1) / V * V);
+        a.slice_w = pl.slice_w;
+        a.rows_per_cluster = pl.rows_per_cluster;
+        a.stages = pl.stages;
+        a.b_buf = w.b_buf;
+        a.b_buf_w = w.b_buf;
+        a.b_off = b_off;
+        a.logcs = w.logcs;
+        a.a = w.a;
+        a.a_off = a_off;
+        a.partials = w.partials;
+        a.n_pad = w.n_pad;
+        a.st = w.st;
+        return a;
+    };
+    auto finalize = [&](int nparts) -> fugal_status {
+        LaunchScope scope(FUGAL_KERNEL_FINALIZE, stream);
+        finalize_kernel<<<fin_blocks, 256, 0, stream>>>(w.partials, nparts, w.n_pad, static_cast<int>(n), w.logcs,
+                                                        w.st);
+        return launch_check("sinkhorn: finalize");
+    };
+
+    // ---- main phase: sweeps t = 0 .. max_iterations-1, polled at evaluation points
+    if (g_pinned_ring == nullptr) {
+        void* ptr = nullptr;
+        FUGAL_TRY(cuda_check(cudaHostAlloc(&ptr, kPinnedSlots * sizeof(int), cudaHostAllocPortable),
+                             "sinkhorn: pinned flags"));
+        g_pinned_ring = static_cast<int*>(ptr);
+    }
+    int* g_pinned_done = g_pinned_ring + g_pinned_next;
+    g_pinned_next = (g_pinned_next + 2) % kPinnedSlots;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    FUGAL_TRY(cuda_check(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), "sinkhorn: event"));
+    FUGAL_TRY(cuda_check(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), "sinkhorn: event"));
+    auto destroy = [&]() {
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+    };
+    int slot = 0;
+    bool pending[2] = {false, false};
+    fugal_status status = FUGAL_OK;
+    for (int t = 0; t < p.max_iterations && status == FUGAL_OK; ++t) {
+        const int snap_idx = (!use16 || t < p.fp32_warmup_sweeps) ? -1 : ((t - p.fp32_warmup_sweeps) / p.reabsorb_every);
+        const bool absorb = use16 && t >= p.fp32_warmup_sweeps && (t - p.fp32_warmup_sweeps) % p.reabsorb_every == 0;
+        if (!use16 || t < p.fp32_warmup_sweeps) {
+            SweepArgs a = sweep_args(plan32, p.cost32, p.ld32, nullptr, nullptr);
+            status = launch_sweep(plan32, kernel_for(plan32.threads, FUGAL_F32, 0), a, stream, FUGAL_KERNEL_SWEEP_F32);
+            if (status == FUGAL_OK) status = finalize(plan32.clusters);
+        } else if (absorb) {
+            // reads cost32 in the FP32 frame (offsets of the previous snapshot if any), writes snapshot snap_idx
+            const float* b_off = snap_idx > 0 ? w.b_snap + ((snap_idx - 1) & 1) * w.n_pad : nullptr;
+            const float* a_off = snap_idx > 0 ? w.a_snap + ((snap_idx - 1) & 1) * w.n_pad : nullptr;
+            SweepArgs a = sweep_args(plan_abs, p.cost32, p.ld32, b_off, a_off);
+            a.out16 = p.cost16;
+            a.ld16 = p.ld16;
+            a.a_snap = w.a_snap + (snap_idx & 1) * w.n_pad;
+            a.b_snap = w.b_snap + (snap_idx & 1) * w.n_pad;
+            status = launch_sweep(plan_abs, kernel_for(plan_abs.threads, FUGAL_F32, p.stream_dtype == FUGAL_BF16 ? 1 : 2),
+                                  a, stream, FUGAL_KERNEL_ABSORB);
+            if (status == FUGAL_OK) status = finalize(plan_abs.clusters);
+        } else {
+            SweepArgs a = sweep_args(plan16, p.cost16, p.ld16, nullptr, nullptr);
+            status = launch_sweep(plan16, kernel_for(plan16.threads, p.stream_dtype, 0), a, stream, FUGAL_KERNEL_SWEEP);
+            if (status == FUGAL_OK) status = finalize(plan16.clusters);
+        }
+        if (status != FUGAL_OK) break;
+        const bool eval_point = (t % p.eval_freq == 0 && t != 0);
+        if (eval_point) {
+            status = cuda_check(cudaMemcpyAsync(&g_pinned_done[slot], &w.st->done, sizeof(int),
+                                                cudaMemcpyDeviceToHost, stream),
+                                "sinkhorn: poll copy");
+            if (status == FUGAL_OK) status = cuda_check(cudaEventRecord(ev[slot], stream), "sinkhorn: poll event");
+            pending[slot] = true;
+            const int other = slot ^ 1;
+            if (status == FUGAL_OK && pending[other]) {
+                status = cuda_check(cudaEventSynchronize(ev[other]), "sinkhorn: poll wait");
+                pending[other] = false;
+                timing_poll();
+                if (status == FUGAL_OK && g_pinned_done[other]) break;
+            }
+            slot = other;
+        }
+    }
+    if (status != FUGAL_OK) {
+        destroy();
+        return status;
+    }
+
+    // ---- polish: FP32 sweeps on cost32 after a reduced-precision phase
+    const int nblk = fin_blocks;
+    if (use16 && p.polish_sweeps > 0) {
+        {
+            LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
+            polish_begin_kernel<<<nblk, 256, 0, stream>>>(w.st, w.a, w.b_buf, w.n_pad, w.logcs, w.a_snap, w.b_snap,
+                                                          static_cast<int>(n), frame);
+            status = launch_check("sinkhorn: polish begin");
+        }
+        for (int k = 0; k < p.polish_sweeps && status == FUGAL_OK; ++k) {
+            SweepArgs a = sweep_args(plan32, p.cost32, p.ld32, nullptr, nullptr);
+            status = launch_sweep(plan32, kernel_for(plan32.threads, FUGAL_F32, 0), a, stream, FUGAL_KERNEL_SWEEP_F32);
+            if (status == FUGAL_OK) status = finalize(plan32.clusters);
+        }
+    }
+    if (status == FUGAL_OK) {
+        LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
+        solve_end_kernel<<<nblk, 256, 0, stream>>>(w.st, w.a, w.b_buf, w.n_pad, w.a_snap, w.b_snap,
+                                                   static_cast<int>(n), frame, p.u_out, p.v_out,
+                                                   static_cast<fugal_solve_record*>(p.record));
+        status = launch_check("sinkhorn: solve end");
+    }
+    destroy();
+    return status;
+}

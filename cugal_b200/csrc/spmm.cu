@@ -1,0 +1,278 @@
+// Sparse adjacency products for the Frank-Wolfe gradient (cugal/pred.py:54-74,
+// cugal/adjacency.py:128-156, cuda_kernels/adjacency.cu:77-150).
+//
+// The reference builds the gradient of the symmetric case as
+// B.mul(A.mul(P).T).T * -2 with two cuSPARSE SpMM calls (a handle, a value
+// vector and a buffer allocated per call), then adds the distance and the
+// lambda term in two more n^2 passes.  Here:
+//
+//   kernel 1:  T = A P, each output tile transposed through shared memory on
+//              the way out, so Tt = (A P)^T is row-major;
+//   kernel 2:  Y = B Tt = (A P B)^T (A, B symmetric), transposed back in
+//              shared memory, and the epilogue writes
+//              out = s * (-2 APB + ||Fs_i - Ft_j|| + c lambda (1 - 2P)) + U_i + V_j
+//              in one pass (distance recomputed from the 4 feature columns, no
+//              n^2 distance matrix is ever stored).
+//
+// Both kernels gather rows of the dense operand with warp-wide 512-byte float4
+// loads.  The grid walks output tiles panel-major (blockIdx.x = row tile,
+// blockIdx.y = 128-column panel), so the CTAs in flight share one panel of the
+// dense operand (n x 128 x 4 bytes, 16 MB at n = 32768) and the gathers hit L2.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "fugal_common.cuh"
+#include "fugal_host.h"
+
+namespace fugal {
+
+constexpr int kTileRows = 32;     // gathered output rows per CTA
+constexpr int kTileCols = 128;    // columns per CTA (32 lanes x float4)
+constexpr int kSpmmThreads = 256; // 8 warps, 4 rows each
+
+// acc = sum over k in N(row) of X[k][c0 .. c0+3] (float4 per lane).
+__device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const int* __restrict__ col,
+                                             const float* __restrict__ X, long long ldx, int row, int c,
+                                             bool c_ok) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int lane = threadIdx.x & 31;
+    const int rs = rp[row], re = rp[row + 1];
+    for (int e = rs; e < re; e += 32) {
+        const int cnt = min(32, re - e);
+        const int idx = (lane < cnt) ? col[e + lane] : 0;
+        int q = 0;
+        for (; q + 4 <= cnt; q += 4) {
+            const int k0 = __shfl_sync(0xffffffffu, idx, q);
+            const int k1 = __shfl_sync(0xffffffffu, idx, q + 1);
+            const int k2 = __shfl_sync(0xffffffffu, idx, q + 2);
+            const int k3 = __shfl_sync(0xffffffffu, idx, q + 3);
+            if (c_ok) {
+                const float4 v0 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k0) * ldx + c));
+                const float4 v1 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k1) * ldx + c));
+                const float4 v2 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k2) * ldx + c));
+                const float4 v3 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k3) * ldx + c));
+                acc.x += v0.x; acc.y += v0.y; acc.z += v0.z; acc.w += v0.w;
+                acc.x += v1.x; acc.y += v1.y; acc.z += v1.z; acc.w += v1.w;
+                acc.x += v2.x; acc.y += v2.y; acc.z += v2.z; acc.w += v2.w;
+                acc.x += v3.x; acc.y += v3.y; acc.z += v3.z; acc.w += v3.w;
+            }
+        }
+        for (; q < cnt; ++q) {
+            const int k = __shfl_sync(0xffffffffu, idx, q);
+            if (c_ok) {
+                const float4 v = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k) * ldx + c));
+                acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+            }
+        }
+    }
+    return acc;
+}
+
+// Fill tile[r][0..127] with the gathered rows r0 .. r0+31 of A X for columns c0 .. c0+127.
+__device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const int* __restrict__ col,
+                                            const float* __restrict__ X, long long ldx, int n, int r0, int c0,
+                                            float (*tile)[kTileCols + 1], float sign) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = c0 + lane * 4;
+    const bool c_ok = c < n;
+    for (int rr = warp; rr < kTileRows; rr += kSpmmThreads / 32) {
+        const int row = r0 + rr;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (row < n) acc = gather_row(rp, col, X, ldx, row, c, c_ok);
+        tile[rr][lane * 4 + 0] = sign * acc.x;
+        tile[rr][lane * 4 + 1] = sign * acc.y;
+        tile[rr][lane * 4 + 2] = sign * acc.z;
+        tile[rr][lane * 4 + 3] = sign * acc.w;
+    }
+}
+
+// Tt[c][r] = (A X)[r][c]  (transposed store), or out[r][c] = sign (A X)[r][c] (direct store).
+__global__ void __launch_bounds__(kSpmmThreads) spmm_kernel(const int* __restrict__ rp, const int* __restrict__ col,
+                                                            const float* __restrict__ X, long long ldx, int n,
+                                                            float* __restrict__ out, long long ldo, int transpose,
+                                                            float sign) {
+    __shared__ float tile[kTileRows][kTileCols + 1];
+    const int r0 = blockIdx.x * kTileRows;
+    const int c0 = blockIdx.y * kTileCols;
+    gather_tile(rp, col, X, ldx, n, r0, c0, tile, sign);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (transpose) {
+        // row c of out gets the 32 values tile[0..31][c - c0]
+        for (int cc = warp; cc < kTileCols; cc += kSpmmThreads / 32) {
+            const int cg = c0 + cc, rg = r0 + lane;
+            if (cg < n && rg < n) out[static_cast<size_t>(cg) * ldo + rg] = tile[lane][cc];
+        }
+    } else {
+        for (int rr = warp; rr < kTileRows; rr += kSpmmThreads / 32) {
+            const int rg = r0 + rr;
+            if (rg >= n) continue;
+            for (int cc = lane; cc < kTileCols; cc += 32) {
+                const int cg = c0 + cc;
+                if (cg < n) out[static_cast<size_t>(rg) * ldo + cg] = tile[rr][cc];
+            }
+        }
+    }
+}
+
+struct EpilogueArgs {
+    const float* P;
+    long long ldp;
+    const float* fs;  // n x 4 (nullable)
+    const float* ft;
+    const float* D;   // stored distances (nullable; used when fs is null)
+    long long ldd;
+    double lam;       // lambda * lambda_scale
+    double out_scale;
+    const double* U;  // nullable
+    const double* V;
+    float* out;
+    long long ldo;
+};
+
+// Y = B Tt = (APB)^T over the tile (rows j0.., cols i0..), then the gradient
+// epilogue in (i, j) orientation.
+__global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __restrict__ rp,
+                                                                const int* __restrict__ col,
+                                                                const float* __restrict__ Tt, long long ldt, int n,
+                                                                const EpilogueArgs ep) {
+    __shared__ float tile[kTileRows][kTileCols + 1];
+    __shared__ float4 fi[kTileCols];
+    __shared__ float4 fj[kTileRows];
+    const int j0 = blockIdx.x * kTileRows;   // gathered rows: target nodes j
+    const int i0 = blockIdx.y * kTileCols;   // lanes: source nodes i
+    const bool has_f = ep.fs != nullptr;
+    if (has_f) {
+        for (int q = threadIdx.x; q < kTileCols; q += kSpmmThreads)
+            fi[q] = (i0 + q < n) ? reinterpret_cast<const float4*>(ep.fs)[i0 + q] : make_float4(0, 0, 0, 0);
+        for (int q = threadIdx.x; q < kTileRows; q += kSpmmThreads)
+            fj[q] = (j0 + q < n) ? reinterpret_cast<const float4*>(ep.ft)[j0 + q] : make_float4(0, 0, 0, 0);
+    }
+    gather_tile(rp, col, Tt, ldt, n, j0, i0, tile, 1.0f);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = j0 + lane;
+    if (j >= n) return;
+    const double vj = ep.V ? ep.V[j] : 0.0;
+    const float4 f2 = has_f ? fj[lane] : make_float4(0, 0, 0, 0);
+    for (int ii = warp; ii < kTileCols; ii += kSpmmThreads / 32) {
+        const int i = i0 + ii;
+        if (i >= n) break;
+        const double apb = static_cast<double>(tile[lane][ii]);
+        const double p = static_cast<double>(ep.P[static_cast<size_t>(i) * ep.ldp + j]);
+        double g = -2.0 * apb + ep.lam * (1.0 - 2.0 * p);
+        if (has_f) {
+            const float4 f1 = fi[ii];
+            const double d0 = (double)f1.x - (double)f2.x, d1 = (double)f1.y - (double)f2.y;
+            const double d2 = (double)f1.z - (double)f2.z, d3 = (double)f1.w - (double)f2.w;
+            g += sqrt(d0 * d0 + d1 * d1 + d2 * d2 + d3 * d3);
+        } else if (ep.D != nullptr) {
+            g += static_cast<double>(ep.D[static_cast<size_t>(i) * ep.ldd + j]);
+        }
+        const double ui = ep.U ? ep.U[i] : 0.0;
+        ep.out[static_cast<size_t>(i) * ep.ldo + j] = static_cast<float>(ep.out_scale * g + ui + vj);
+    }
+}
+
+// out^T[j][i] = sign * sum_{k in N(i)} Q[j][k]  (M = Q^T operand of the reference's adjacency_matmul)
+__global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const int* __restrict__ col,
+                                               const float* __restrict__ Q, long long ldq, int n,
+                                               float* __restrict__ outT, long long ldo, float sign) {
+    const int i = blockIdx.y * blockDim.x + threadIdx.x;
+    const int j = blockIdx.x;
+    if (i >= n) return;
+    float acc = 0.f;
+    const float* qrow = Q + static_cast<size_t>(j) * ldq;
+    for (int e = rp[i]; e < rp[i + 1]; ++e) acc += qrow[col[e]];
+    outT[static_cast<size_t>(j) * ldo + i] = sign * acc;
+}
+
+fugal_status check_csr(const int32_t* rp, const int32_t* col, int64_t n, const char* who) {
+    if (rp == nullptr || col == nullptr) return fail(FUGAL_BAD_ARGUMENT, "%s: null CSR pointer", who);
+    if (n <= 0 || n > (1ll << 30)) return fail(FUGAL_BAD_SHAPE, "%s: bad n", who);
+    return FUGAL_OK;
+}
+
+}  // namespace fugal
+
+using namespace fugal;
+
+extern "C" fugal_status fugal_adjacency_matmul(const int32_t* col_indices, const int32_t* row_pointers, int64_t n,
+                                               const float* M, int64_t ldm, int m_transposed, float* out,
+                                               int64_t ldo, int negate, fugal_stream_t stream_) {
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    FUGAL_TRY(check_csr(row_pointers, col_indices, n, "fugal_adjacency_matmul"));
+    if (M == nullptr || out == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_adjacency_matmul: null matrix");
+    if (ldm < n || ldo < n) return fail(FUGAL_BAD_SHAPE, "fugal_adjacency_matmul: leading dimension < n");
+    const float sign = negate ? -1.f : 1.f;
+    LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
+    if (!m_transposed) {
+        if ((ldm % 4) != 0 || !aligned16(M))
+            return fail(FUGAL_BAD_SHAPE, "fugal_adjacency_matmul: M needs ld %% 4 == 0 and a 16-byte base");
+        dim3 grid(static_cast<unsigned>((n + kTileRows - 1) / kTileRows),
+                  static_cast<unsigned>((n + kTileCols - 1) / kTileCols));
+        spmm_kernel<<<grid, kSpmmThreads, 0, stream>>>(row_pointers, col_indices, M, ldm, static_cast<int>(n), out,
+                                                        ldo, 0, sign);
+    } else {
+        dim3 grid(static_cast<unsigned>(n), static_cast<unsigned>((n + 127) / 128));
+        spmm_transposed_operand_kernel<<<grid, 128, 0, stream>>>(row_pointers, col_indices, M, ldm,
+                                                                 static_cast<int>(n), out, ldo, sign);
+    }
+    return launch_check("fugal_adjacency_matmul");
+}
+
+extern "C" fugal_status fugal_gradient_workspace_size(int64_t n, size_t* bytes) {
+    if (bytes == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_gradient_workspace_size: null output");
+    if (n <= 0) return fail(FUGAL_BAD_SHAPE, "fugal_gradient_workspace_size: n must be positive");
+    const int64_t ldt = (n + 3) / 4 * 4;
+    *bytes = static_cast<size_t>(n) * ldt * sizeof(float);
+    return FUGAL_OK;
+}
+
+extern "C" fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices,
+                                          const int32_t* b_row_pointers, const int32_t* b_col_indices,
+                                          const float* P, int64_t ldp, const float* source_features,
+                                          const float* target_features, const float* D, int64_t ldd,
+                                          double lambda, double lambda_scale, double out_scale, const double* U,
+                                          const double* V, float* out, int64_t ldo, void* workspace,
+                                          size_t workspace_bytes, fugal_stream_t stream_) {
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    FUGAL_TRY(check_csr(a_row_pointers, a_col_indices, n, "fugal_fw_gradient(A)"));
+    FUGAL_TRY(check_csr(b_row_pointers, b_col_indices, n, "fugal_fw_gradient(B)"));
+    if (P == nullptr || out == nullptr || workspace == nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_fw_gradient: null pointer");
+    if ((source_features == nullptr) != (target_features == nullptr))
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_fw_gradient: give both feature matrices or neither");
+    if ((U == nullptr) != (V == nullptr)) return fail(FUGAL_BAD_ARGUMENT, "fugal_fw_gradient: give both U and V");
+    if (source_features != nullptr && D != nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_fw_gradient: give features or a distance matrix, not both");
+    if (D != nullptr && ldd < n) return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: ldd < n");
+    if (ldp < n || ldo < n || (ldp % 4) != 0 || !aligned16(P))
+        return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: P needs ld >= n, ld %% 4 == 0, 16-byte base");
+    if (source_features && (!aligned16(source_features) || !aligned16(target_features)))
+        return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: feature rows must be 16-byte aligned");
+    size_t need = 0;
+    FUGAL_TRY(fugal_gradient_workspace_size(n, &need));
+    if (workspace_bytes < need || !aligned16(workspace))
+        return fail(FUGAL_WORKSPACE_TOO_SMALL, "fugal_fw_gradient: workspace %zu < %zu bytes", workspace_bytes, need);
+    float* Tt = static_cast<float*>(workspace);
+    const int64_t ldt = (n + 3) / 4 * 4;
+    dim3 grid(static_cast<unsigned>((n + kTileRows - 1) / kTileRows),
+              static_cast<unsigned>((n + kTileCols - 1) / kTileCols));
+    {
+        LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
+        spmm_kernel<<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp, static_cast<int>(n), Tt,
+                                                        ldt, 1, 1.f);
+        FUGAL_TRY(launch_check("fugal_fw_gradient: A P"));
+    }
+    EpilogueArgs ep{P, ldp, source_features, target_features, D, ldd, lambda * lambda_scale, out_scale, U, V, out,
+                    ldo};
+    {
+        LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
+        gradient_kernel<<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt, ldt,
+                                                            static_cast<int>(n), ep);
+        FUGAL_TRY(launch_check("fugal_fw_gradient: (A P) B + epilogue"));
+    }
+    return FUGAL_OK;
+}

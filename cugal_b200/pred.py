@@ -1,0 +1,264 @@
+"""FUGAL alignment driver (reference ``cugal/pred.py``), drop-in ``cugal()``.
+
+``cugal(source, target, config, profile)`` has the reference's signature and
+return value ``(P as a host numpy array, [(i, column_i)])``.  The Frank-Wolfe
+loop (``pred.py:89-148``) runs as three kernel-library calls per step, all
+asynchronous on the current CUDA stream:
+
+  gradient  ``fugal_fw_gradient``    -2 A P B + D + lambda (1 - 2P), written as the
+                                      absorbed Sinkhorn input K + U_i + V_j
+  solve     ``fugal_sinkhorn_solve``  whole log-domain solve, decisions on device
+  update    ``fugal_fw_update``       P += alpha (q - P), FP64 duality gap, duals folded
+
+The host only waits inside a solve (to stop enqueuing sweeps after
+convergence) and, when ``frank_wolfe_threshold`` is set, for the gap.  Only
+CUDA devices are supported; a CPU config raises.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.optimize
+import scipy.sparse
+import scipy.sparse.csgraph
+import torch
+
+from . import _native as N
+from .adjacency import Adjacency
+from .config import Config, HungarianMethod, SinkhornMethod
+from .feature_extraction import Features
+from .greedy_lap import greedy_assign
+from .profile import Phase, Profile, SinkhornProfile, TimeStamp
+from .sinkhorn import SinkhornSolver, padded_ld, read_record
+
+
+def check_config(config: Config) -> None:
+    if "cuda" not in str(config.device):
+        raise ValueError("cugal_b200 runs on CUDA devices only (config.device must be 'cuda[:k]')")
+    if config.sinkhorn_method != SinkhornMethod.LOG:
+        raise NotImplementedError(f"sinkhorn_method={config.sinkhorn_method.value} is not available; use LOG")
+    if config.dtype != torch.float32:
+        raise NotImplementedError("config.dtype must be torch.float32 on the GPU path "
+                                  "(set stream_dtype for BF16/FP16 streaming)")
+    if config.stream_dtype not in N.STREAM_DTYPES:
+        raise ValueError(f"unsupported stream_dtype {config.stream_dtype}")
+
+
+@dataclass
+class FrankWolfeEngine:
+    """Device state of one alignment: P, the absorbed cost, duals, workspaces."""
+
+    A: Adjacency
+    B: Adjacency
+    features: Features | torch.Tensor
+    config: Config
+    max_solves: int = 0
+    n: int = field(init=False)
+
+    def __post_init__(self):
+        n = self.A.number_of_nodes()
+        if self.B.number_of_nodes() != n:
+            raise ValueError("source and target must have the same number of nodes")
+        self.n = n
+        dev = torch.device(self.config.device)
+        self.device = dev
+        self.ld = padded_ld(n)
+        self.P_buf = torch.zeros((n, self.ld), dtype=torch.float32, device=dev)
+        self.P_buf[:, :n] = 1.0 / n
+        self.cost32 = torch.empty((n, self.ld), dtype=torch.float32, device=dev)
+        self.U = torch.zeros(n, dtype=torch.float64, device=dev)
+        self.V = torch.zeros(n, dtype=torch.float64, device=dev)
+        self.u = torch.zeros(n, dtype=torch.float32, device=dev)
+        self.v = torch.zeros(n, dtype=torch.float32, device=dev)
+        self.gap = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.grad_ws = torch.empty(N.workspace_size("fugal_gradient_workspace_size", n), dtype=torch.uint8,
+                                   device=dev)
+        self.solver = SinkhornSolver(n, self.config, dev)
+        self.records = torch.empty((max(1, self.max_solves), N.RECORD_BYTES), dtype=torch.uint8, device=dev)
+        self.solves = 0
+        if isinstance(self.features, Features):
+            self.fs = self.features.source.float().contiguous()
+            self.ft = self.features.target.float().contiguous()
+            self.D = None
+        else:
+            self.fs = self.ft = None
+            self.D = self.features.float().contiguous()
+        # dense reference path adds the lambda term twice (cugal/pred.py:46-50)
+        self.lambda_scale = 1.0 if self.config.use_sparse_adjacency else 2.0
+
+    @property
+    def P(self) -> torch.Tensor:
+        return self.P_buf[:, :self.n]
+
+    def gradient(self, lam: float, out_scale: float | None = None, out: torch.Tensor | None = None,
+                 absorbed: bool = True) -> torch.Tensor:
+        reg = self.config.sinkhorn_regularization
+        out = self.cost32 if out is None else out
+        scale = (-1.0 / reg) if out_scale is None else out_scale
+        N.call("fugal_fw_gradient", self.n, self.A.row_pointers.data_ptr(), self.A.col_indices.data_ptr(),
+               self.B.row_pointers.data_ptr(), self.B.col_indices.data_ptr(), self.P_buf.data_ptr(), self.ld,
+               N.ptr(self.fs), N.ptr(self.ft), N.ptr(self.D), self.n if self.D is not None else 0,
+               float(lam), self.lambda_scale, scale, N.ptr(self.U) if absorbed else None,
+               N.ptr(self.V) if absorbed else None, out.data_ptr(), N.matrix_ld(out, "out"),
+               self.grad_ws.data_ptr(), self.grad_ws.numel(), N.stream_handle(self.device))
+        return out
+
+    def solve(self) -> int:
+        k = self.solves
+        if k >= self.records.shape[0]:
+            self.records = torch.cat([self.records, torch.empty_like(self.records)])
+        self.solver.solve(self.cost32, self.u, self.v, self.records[k].data_ptr())
+        self.solves += 1
+        return k
+
+    def update(self, alpha: float) -> torch.Tensor:
+        N.call("fugal_fw_update", self.n, self.P_buf.data_ptr(), self.ld, self.cost32.data_ptr(), self.ld,
+               self.u.data_ptr(), self.v.data_ptr(), self.U.data_ptr(), self.V.data_ptr(), float(alpha),
+               float(self.config.sinkhorn_regularization), self.gap.data_ptr(), 1, N.stream_handle(self.device))
+        return self.gap
+
+    def sinkhorn_profiles(self) -> list[SinkhornProfile]:
+        raw = self.records[:self.solves].cpu()
+        return [read_record(raw[k]) for k in range(self.solves)]
+
+
+def sparse_gradient(A: Adjacency, B: Adjacency, A_transpose, B_transpose, P: torch.Tensor,
+                    features: Features | torch.Tensor, iteration: int) -> torch.Tensor:
+    """Plain gradient -2 A P B + D + iteration (1 - 2P) (``cugal/pred.py:54-74``), symmetric A, B."""
+    if A is not A_transpose or B is not B_transpose:
+        raise NotImplementedError("only undirected graphs (symmetric adjacency) are supported")
+    config = Config(device=str(P.device), dtype=torch.float32, sinkhorn_method=SinkhornMethod.LOG,
+                    use_sparse_adjacency=True)
+    eng = FrankWolfeEngine(A, B, features, config)
+    eng.P_buf[:, :eng.n] = P
+    return eng.gradient(iteration, out_scale=1.0, out=torch.empty_like(eng.P_buf), absorbed=False)[:, :eng.n]
+
+
+GREEDY_METHODS = (HungarianMethod.GREEDY, HungarianMethod.DOUBLE_GREEDY, HungarianMethod.PARALLEL_GREEDY,
+                  HungarianMethod.RAND)
+
+
+def round_on_device(P: torch.Tensor, config: Config, profile: Profile):
+    """Sparsity count and rounding; returns (count tensor, columns as a device
+    tensor for the greedy methods or a host array for the scipy methods)."""
+    n = P.shape[0]
+    count = torch.zeros(1, dtype=torch.int64, device=P.device)
+    N.call("fugal_count_le", P.data_ptr(), N.matrix_ld(P, "P"), n, float(torch.finfo(P.dtype).eps),
+           count.data_ptr(), N.stream_handle(P.device))
+    start_time = TimeStamp(config.device)
+    method = config.hungarian_method
+    if method == HungarianMethod.SCIPY:
+        _, cols = scipy.optimize.linear_sum_assignment(P.cpu().numpy(), maximize=True)
+    elif method in GREEDY_METHODS:
+        cols = greedy_assign(P, method, config.lap_candidates)
+    elif method == HungarianMethod.SPARSE:
+        host = scipy.sparse.csr_matrix(P.cpu().numpy())
+        _, cols = scipy.sparse.csgraph.min_weight_full_bipartite_matching(host, maximize=True)
+    else:
+        raise NotImplementedError(f"hungarian_method={method.value} is not available on the GPU path")
+    profile.log_time(start_time, Phase.HUNGARIAN)
+    return count, cols
+
+
+def hungarian(quasi_permutation: torch.Tensor, config: Config, profile: Profile) -> np.ndarray:
+    """Rounding step (``cugal/pred.py:151-178``)."""
+    n = quasi_permutation.shape[0]
+    count, cols = round_on_device(quasi_permutation, config, profile)
+    if isinstance(cols, torch.Tensor):
+        cols = cols.cpu().numpy()
+    profile.sparsity = int(count.item()) / (n * n)
+    return cols
+
+
+def convert_to_permutation_matrix(quasi_permutation: torch.Tensor, config: Config,
+                                  profile: Profile) -> tuple[np.ndarray, list[tuple[int, int]]]:
+    """(P on the host, [(i, col[i])]) (``cugal/pred.py:181-193``)."""
+    cols = hungarian(quasi_permutation, config, profile)
+    mapping = [(i, int(c)) for i, c in enumerate(cols)]
+    return quasi_permutation.cpu().numpy(), mapping
+
+
+def find_quasi_permutation_matrix(A: Adjacency, B: Adjacency, features: Features | torch.Tensor,
+                                  config: Config, profile: Profile) -> torch.Tensor:
+    """Frank-Wolfe loop (``cugal/pred.py:89-148``)."""
+    check_config(config)
+    engine = FrankWolfeEngine(A, B, features, config, max_solves=config.iter_count * config.frank_wolfe_iter_count)
+    solve_times = []
+    for lam in range(config.iter_count):
+        for it in range(1, config.frank_wolfe_iter_count + 1):
+            start_time = TimeStamp(config.device)
+            engine.gradient(lam)
+            profile.log_time(start_time, Phase.GRADIENT)
+
+            start_time = TimeStamp(config.device)
+            engine.solve()
+            end_time = TimeStamp(config.device)
+            solve_times.append((start_time, end_time))
+            profile.log_time(start_time, Phase.SINKHORN)
+
+            alpha = 2.0 / float(2.0 + it)
+            gap = engine.update(alpha)
+            profile.frank_wolfe_iterations += 1
+            if config.frank_wolfe_threshold is not None and abs(float(gap.item())) < config.frank_wolfe_threshold:
+                break
+    for (s, e), sp in zip(solve_times, engine.sinkhorn_profiles()):
+        sp.time = e.elapsed_seconds(s)
+        profile.sinkhorn_profiles.append(sp)
+    if config.safe_mode:
+        assert engine.P.isfinite().all(), "quasi_permutation tensor has NaN values"
+    return engine.P
+
+
+def pad_graphs(source, target) -> None:
+    """Node padding of ``cugal()`` (``cugal/pred.py:209-212``), including its use of
+    range(max label), which leaves the larger label itself to the graph that has it."""
+    node_count = max(max(source.nodes()), max(target.nodes()))
+    source.add_nodes_from(set(range(node_count)) - set(source.nodes()))
+    target.add_nodes_from(set(range(node_count)) - set(target.nodes()))
+
+
+def align(A: Adjacency, B: Adjacency, config: Config, profile: Profile | None = None):
+    """Whole alignment on device-resident CSR graphs: features, Frank-Wolfe,
+    rounding.  Returns (P view, columns, sparsity-count tensor) without any
+    device-to-host copy for the greedy rounding methods."""
+    check_config(config)
+    profile = Profile() if profile is None else profile
+    start_time = TimeStamp(config.device)
+    features = Features.create(A, B, config)
+    profile.log_time(start_time, Phase.FEATURE_EXTRACTION)
+    P = find_quasi_permutation_matrix(A, B, features, config, profile)
+    count, cols = round_on_device(P, config, profile)
+    return P, cols, count
+
+
+def cugal(source, target, config: Config, profile: Profile | None = None
+          ) -> tuple[np.ndarray, list[tuple[int, int]]]:
+    """Run the alignment (``cugal/pred.py:196-249``).
+
+    Returns the quasi-permutation matrix (host numpy, FP32) and the mapping from
+    source to target node.  ``profile`` is filled in place; unlike the reference,
+    the default is a fresh Profile per call rather than one shared default."""
+    check_config(config)
+    profile = Profile() if profile is None else profile
+    before = time.time()
+    pad_graphs(source, target)
+    A = Adjacency.from_graph(source, config.device)
+    B = Adjacency.from_graph(target, config.device)
+
+    start_time = TimeStamp(config.device)
+    features = Features.create(A, B, config)
+    profile.log_time(start_time, Phase.FEATURE_EXTRACTION)
+
+    quasi_permutation = find_quasi_permutation_matrix(A, B, features, config, profile)
+    output = convert_to_permutation_matrix(quasi_permutation, config, profile)
+    if config.safe_mode:
+        assert np.isfinite(output[0]).all(), "output permutation matrix has NaN values"
+    profile.resolve()
+    profile.time = time.time() - before
+    dev = torch.device(config.device)
+    profile.max_memory = torch.cuda.max_memory_allocated(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    return output

@@ -1,0 +1,244 @@
+/*
+ * fugal_b200.h -- C ABI of the B200 (sm_100a) FUGAL alignment kernels.
+ *
+ * Plain pointers and sizes only: every matrix/vector argument is a DEVICE
+ * pointer owned by the caller (row-major, leading dimension in elements), every
+ * call is asynchronous on the given CUDA stream and returns a fugal_status.
+ * No entry point synchronises the device or allocates device memory; kernels
+ * that need scratch take a caller-provided workspace whose size is returned by
+ * the matching *_workspace_size() query.  A non-OK status leaves a message in
+ * fugal_last_error().
+ *
+ * The first group mirrors, one entry point each, the pybind11 module
+ * `cuda_kernels` of cuGAL (cuda_kernels/kernels.cpp:4-30, bound at :32-70) that
+ * cugal/*.py calls.  The second group is the fused path that replaces the
+ * Python-level Frank-Wolfe step (cugal/pred.py:89-148) with three calls:
+ * gradient -> Sinkhorn solve -> update.
+ */
+#ifndef FUGAL_B200_H
+#define FUGAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* fugal_stream_t; /* == cudaStream_t; NULL = legacy default stream */
+
+typedef enum {
+    FUGAL_OK = 0,
+    FUGAL_BAD_SHAPE = 1,        /* size, leading dimension or alignment not supported */
+    FUGAL_BAD_ARGUMENT = 2,     /* null pointer, bad enum value, bad parameter */
+    FUGAL_CUDA_ERROR = 3,       /* a CUDA runtime call failed (launch, attribute, event) */
+    FUGAL_ITER_LIMIT = 4,       /* an iteration cap was hit where that is an error */
+    FUGAL_NONFINITE = 5,        /* NaN / Inf detected */
+    FUGAL_DEVICE_TIMEOUT = 6,   /* a bounded device-side wait gave up (kernel returned early) */
+    FUGAL_WORKSPACE_TOO_SMALL = 7,
+    FUGAL_UNSUPPORTED = 8
+} fugal_status;
+
+typedef enum { FUGAL_F32 = 0, FUGAL_BF16 = 1, FUGAL_F16 = 2 } fugal_dtype;
+
+typedef enum {
+    FUGAL_LAP_GREEDY = 0,          /* cugal/greedy_lap.py:10-19 */
+    FUGAL_LAP_DOUBLE_GREEDY = 1,   /* cugal/greedy_lap.py:50-63 */
+    FUGAL_LAP_PARALLEL_GREEDY = 2, /* cugal/greedy_lap.py:65-85 */
+    FUGAL_LAP_ORDERED = 3          /* RAND: rows in a caller-given order, cugal/greedy_lap.py:21-32 */
+} fugal_lap_method;
+
+/* Kernel families counted / timed by the instrumentation below. */
+typedef enum {
+    FUGAL_KERNEL_SWEEP = 0,       /* fused Sinkhorn sweep over the BF16/FP16 cost copy */
+    FUGAL_KERNEL_SWEEP_F32 = 1,   /* fused Sinkhorn sweep over the FP32 cost (warm-up, polish, FP32 stream) */
+    FUGAL_KERNEL_ABSORB = 2,      /* FP32 sweep that also writes the reduced-precision copy */
+    FUGAL_KERNEL_FINALIZE = 3,    /* per-sweep column reduction + convergence decision */
+    FUGAL_KERNEL_COLUMN_PASS = 4, /* column LSE of the first iteration of a solve */
+    FUGAL_KERNEL_GRADIENT = 5,    /* both SpMM kernels of the gradient */
+    FUGAL_KERNEL_UPDATE = 6,
+    FUGAL_KERNEL_OTHER = 7,
+    FUGAL_KERNEL_FAMILIES = 8
+} fugal_kernel_family;
+
+#define FUGAL_MAX_RECORDED_ERRORS 256
+
+const char* fugal_status_string(int status);
+const char* fugal_last_error(void);
+int fugal_version(void);
+
+/* ======================= mirrors of cuda_kernels (kernels.cpp:4-30) ======= */
+
+/* adjacency_matmul (kernels.cpp:5-7; cuda_kernels/adjacency.cu:77-150).
+ * out = (negate ? -A : A) @ M for the n x n CSR matrix A (int32 indices).
+ * m_transposed == 0: M row-major (ldm), out row-major (ldo).
+ * m_transposed == 1: M is the transpose of a row-major Q (M = Q^T, Q has leading
+ *   dimension ldm) and out is written column-major, i.e. out^T row-major with
+ *   leading dimension ldo -- the strides torch.empty_like(M) gives a transposed
+ *   view, which is what the reference's cuSPARSE call writes (adjacency.cu:93,116). */
+fugal_status fugal_adjacency_matmul(const int32_t* col_indices, const int32_t* row_pointers, int64_t n,
+                                    const float* M, int64_t ldm, int m_transposed, float* out, int64_t ldo,
+                                    int negate, fugal_stream_t stream);
+
+/* create_adjacency (kernels.cpp:8; cuda_kernels/adjacency.cu:228-259).
+ * edges: edge_count int32 pairs (x, y) as cugal/adjacency.py:68-69 flattens
+ * them; row y of the CSR receives column x, columns ascending within a row.
+ * Every row pointer is written, including rows without edges. */
+fugal_status fugal_create_adjacency_workspace_size(int64_t edge_count, int64_t node_count, size_t* bytes);
+fugal_status fugal_create_adjacency(const int32_t* edges, int64_t edge_count, int64_t node_count,
+                                    int32_t* col_indices, int32_t* row_pointers, void* workspace,
+                                    size_t workspace_bytes, fugal_stream_t stream);
+
+/* graph_features (kernels.cpp:11; cuda_kernels/feature_extraction.cu:67-84).
+ * degrees[v] = deg(v); clustering[v] = t(v) / (deg (deg-1)) with
+ * t(v) = sum_{u in N(v)} |N(v) & N(u)| (integer), 0 when t == 0 or deg < 2.
+ * Optional integer outputs: degree_counts (int32) and triangle_counts (t, int64). */
+fugal_status fugal_graph_features(const int32_t* col_indices, const int32_t* row_pointers, int64_t n,
+                                  float* clustering, float* degrees, int32_t* degree_counts,
+                                  int64_t* triangle_counts, fugal_stream_t stream);
+
+/* average_neighbor_features (kernels.cpp:12-14; feature_extraction.cu:108-125).
+ * averages[v] = (FP32 sum of features over N(v) in CSR order) / deg(v), 0 if deg == 0. */
+fugal_status fugal_average_neighbor_features(const int32_t* col_indices, const int32_t* row_pointers,
+                                             int64_t n, const float* features, float* averages,
+                                             fugal_stream_t stream);
+
+/* sinkhorn_log_step (kernels.cpp:17; cuda_kernels/sinkhorn_log.cu:100-114).
+ * out[r] = (1 - w) out[r] - w * LSE_c(K[r, c] + add[c]); |w - 1| < 1e-4 writes -LSE. */
+fugal_status fugal_sinkhorn_log_step(const float* K, int64_t rows, int64_t cols, int64_t ldk,
+                                     const float* add, float* out, float momentum, fugal_stream_t stream);
+
+/* sinkhorn_log_marginal (kernels.cpp:18; cuda_kernels/sinkhorn_log.cu:88-98).
+ * *result = sum over rows (axis 1, as the reference kernel) or columns (axis 0,
+ * as cugal/sinkhorn.py:67-76) of |sum exp(K + u_r + v_c) - 1|, accumulated in FP64
+ * into the DEVICE double `result`. */
+fugal_status fugal_sinkhorn_log_marginal(const float* K, int64_t n, int64_t ldk, const float* u,
+                                         const float* v, int axis, double* result, fugal_stream_t stream);
+
+/* add_distance (kernels.cpp:21; cuda_kernels/distance.cu:35-53).
+ * out[x][y] += ||source[x] - target[y]||_2 over the 4 feature columns (direct differences). */
+fugal_status fugal_add_distance(const float* source, const float* target, int64_t n, float* out,
+                                int64_t ldo, fugal_stream_t stream);
+
+/* regularize (kernels.cpp:24; cuda_kernels/regularize.cu:24-39): G += it - 2 it P. */
+fugal_status fugal_regularize(float* gradient, int64_t ldg, const float* P, int64_t ldp, int64_t n,
+                              int iteration, fugal_stream_t stream);
+
+/* update_quasi_permutation_log (kernels.cpp:27; update_quasi_permutation.cu:37-56).
+ * q = exp(K + u_r + v_c); P += alpha (q - P); *gap = sum (q - P)(-reg K) in FP64
+ * (DEVICE double; the reference returns |gap| to the host). */
+fugal_status fugal_update_quasi_permutation_log(float* P, int64_t ldp, const float* K, int64_t ldk,
+                                                const float* u, const float* v, int64_t n, float alpha,
+                                                float regularization, double* gap, fugal_stream_t stream);
+
+/* Greedy rounding (replaces cugal/greedy_lap.py:7-85, which the reference runs
+ * as n sequential torch launches with a host read each; dense_hungarian,
+ * kernels.cpp:30, is exported but never called by cugal).  columns_out[r] is the
+ * column of row r; with mutate != 0, P is changed as the reference changes it
+ * (row r multiplied by the columns still free when r was processed). order: the
+ * row order for FUGAL_LAP_ORDERED (int64 device array), else ignored. */
+fugal_status fugal_greedy_lap_workspace_size(int64_t n, int candidates, size_t* bytes);
+fugal_status fugal_greedy_lap(float* P, int64_t ldp, int64_t n, int method, const int64_t* order,
+                              int candidates, int mutate, int64_t* columns_out, void* workspace,
+                              size_t workspace_bytes, fugal_stream_t stream);
+
+/* count of entries of P (n x n) that are <= threshold (cugal/pred.py:152-153), into a DEVICE int64. */
+fugal_status fugal_count_le(const float* P, int64_t ldp, int64_t n, float threshold, int64_t* count,
+                            fugal_stream_t stream);
+
+/* ======================= fused Frank-Wolfe step (cugal/pred.py:89-148) ===== */
+
+/* Gradient with the Sinkhorn kernel matrix fused into its epilogue
+ * (cugal/pred.py:54-74 sparse_gradient + add_feature_distance :30-35 +
+ * regularize + K = -C/reg at cugal/sinkhorn.py:98), for symmetric A and B:
+ *   C[i][j]   = -2 (A P B)[i][j] + ||Fs_i - Ft_j|| + lambda_scale * lambda * (1 - 2 P[i][j])
+ *   out[i][j] = out_scale * C[i][j] + U[i] + V[j]          (FP64 arithmetic, FP32 store)
+ * out_scale = -1/reg with U, V the accumulated duals gives the absorbed Sinkhorn
+ * input; out_scale = 1, U = V = NULL gives the plain gradient.  Features are the
+ * n x 4 mu-scaled feature rows; alternatively D (n x n, ldd) is a stored distance
+ * matrix read instead (the reference's recompute_distance=False input); with
+ * neither there is no distance term.  lambda_scale is 1 for
+ * the sparse reference path and 2 for its dense path (cugal/pred.py:46-50). */
+fugal_status fugal_gradient_workspace_size(int64_t n, size_t* bytes);
+fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices,
+                               const int32_t* b_row_pointers, const int32_t* b_col_indices, const float* P,
+                               int64_t ldp, const float* source_features, const float* target_features,
+                               const float* D, int64_t ldd, double lambda, double lambda_scale,
+                               double out_scale, const double* U, const double* V, float* out, int64_t ldo,
+                               void* workspace, size_t workspace_bytes, fugal_stream_t stream);
+
+/* Log-domain Sinkhorn solve (cugal/sinkhorn.py:90-120) on the absorbed cost
+ * cost32 = K + U_i + V_j, warm-started at u = v = 0 relative to that frame.
+ * Same iteration as the reference: per iteration a column then a row update
+ * (Lehmann momentum from sinkhorn_momentum_start), the column-marginal L1 error
+ * checked after iterations eval_freq, 2 eval_freq, ... against threshold, at most
+ * max_iterations iterations.  Each sweep reads the cost once: the row update and
+ * the next column update's sums are fused.  With stream_dtype BF16/F16 the solve
+ * switches, after fp32_warmup_sweeps, to the reduced-precision copy `cost16`
+ * (which it writes, refreshed every reabsorb_every sweeps), then runs
+ * polish_sweeps FP32 sweeps.  Outputs: u_out / v_out (FP32, n) in the frame of
+ * cost32, and an optional DEVICE fugal_solve_record. */
+typedef struct {
+    int64_t n;
+    const float* cost32;
+    int64_t ld32;
+    void* cost16;
+    int64_t ld16;
+    int stream_dtype;
+    int max_iterations;
+    double threshold;
+    int eval_freq;
+    int momentum_start; /* < 0: no momentum (Config.sinkhorn_momentum_start = None) */
+    int fp32_warmup_sweeps;
+    int reabsorb_every;
+    int polish_sweeps;
+    float* u_out;
+    float* v_out;
+    void* record; /* fugal_solve_record* in device memory, or NULL */
+} fugal_solve_params;
+
+typedef struct {
+    int32_t iteration_count; /* iterations of the main phase (SinkhornProfile.iteration_count) */
+    int32_t n_errors;        /* entries of errors[] (SinkhornProfile.errors) */
+    int32_t status;          /* FUGAL_OK or FUGAL_DEVICE_TIMEOUT */
+    int32_t polish_count;
+    double last_error;       /* column-marginal L1 error after the last main-phase sweep */
+    double polish_error;     /* after the polish sweeps (FP32 cost) */
+    double errors[FUGAL_MAX_RECORDED_ERRORS];
+} fugal_solve_record;
+
+fugal_status fugal_sinkhorn_workspace_size(int64_t n, int stream_dtype, size_t* bytes);
+fugal_status fugal_sinkhorn_solve(const fugal_solve_params* params, void* workspace, size_t workspace_bytes,
+                                  fugal_stream_t stream);
+
+/* Frank-Wolfe update (cugal/pred.py:133-141 and update_quasi_permutation.cu:7-35)
+ * on the absorbed cost: q = exp(cost32 + u_i + v_j), P += alpha (q - P),
+ * *gap = sum (q - P) C with C = -reg (cost32 - U_i - V_j) (FP64, DEVICE double).
+ * commit != 0 then folds the duals into the frame: U += u, V += v. */
+fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32,
+                             const float* u, const float* v, double* U, double* V, double alpha,
+                             double regularization, double* gap, int commit, fugal_stream_t stream);
+
+/* ======================= instrumentation ================================== */
+/* When enabled, every kernel of the families above is bracketed by CUDA events
+ * on its launch stream; totals are accumulated when a solve polls its progress
+ * or on fugal_timing_query(), which synchronises the recorded events. */
+void fugal_timing_enable(int on);
+void fugal_timing_reset(void);
+fugal_status fugal_timing_query(int family, int64_t* launches, double* milliseconds);
+/* Kernels launched by this library since load (all families). */
+int64_t fugal_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* FUGAL_B200_H */
