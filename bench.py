@@ -187,6 +187,29 @@ def traffic_per_launch(n: int, ld: int):
     return d["dram_bytes_per_launch"] * (n * ld) / (d["n"] * d["ld"])
 
 
+def reference_gpu_sample(n: int, solves: int, sweeps: float, iters: int = 20):
+    """Seconds per alignment of the reference's FP32 GPU Sinkhorn (its own kernels,
+    oracle/_ref), extrapolated from `iters` timed iterations at size n, or None."""
+    from oracle import ref_gpu
+    if not ref_gpu.available():
+        return None
+    g = torch.Generator(device="cuda").manual_seed(0)
+    C = torch.rand((n, n), generator=g, device="cuda") * 4
+    u = torch.zeros(n, device="cuda")
+    v = torch.zeros(n, device="cuda")
+    ref_gpu.solve_log(C, u, v, 1e-3, 3, 0.0, 10)  # warm-up (includes the transposed copy)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ref_gpu.solve_log(C, u, v, 1e-3, iters, 0.0, 10)
+    torch.cuda.synchronize()
+    per_iter = (time.perf_counter() - t0) / iters
+    del C
+    torch.cuda.empty_cache()
+    return {"value": per_iter * sweeps * solves, "unit": UNIT, "per_iteration_ms": per_iter * 1e3,
+            "sample": f"{iters} iterations of the reference's solve_log GPU loop (cugal/sinkhorn.py:99-116) on its "
+                      f"own kernels at n={n}, extrapolated to {solves} solves x {sweeps:g} iterations"}
+
+
 def run_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
@@ -305,6 +328,14 @@ def run_ours(args):
                                                  args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref_gpu = reference_gpu_sample(n, config.iter_count * config.frank_wolfe_iter_count,
+                                           mean_sweeps or config.sinkhorn_iterations)
+        except Exception as exc:  # the reference build is optional
+            ref_gpu = {"unavailable": str(exc)[:200]}
+
     if rank == 0:
         value = elapsed / args.steps
         line = {
@@ -327,6 +358,7 @@ def run_ours(args):
                          "peak_kind": peak_kind},
             "kernel_times_ms": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in fam.items()},
             "cpu_baseline": cpu,
+            "reference_gpu_fp32": ref_gpu,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "clocks": clk,

@@ -186,7 +186,7 @@ extern "C" fugal_status fugal_graph_features(const int32_t* col_indices, const i
                                              float* clustering, float* degrees, int32_t* degree_counts,
                                              int64_t* triangle_counts, fugal_stream_t stream_) {
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
-    if (col_indices == nullptr || row_pointers == nullptr || clustering == nullptr || degrees == nullptr)
+    if (row_pointers == nullptr || clustering == nullptr || degrees == nullptr)
         return fail(FUGAL_BAD_ARGUMENT, "fugal_graph_features: null argument");
     if (n <= 0 || n > INT_MAX - 1) return fail(FUGAL_BAD_SHAPE, "fugal_graph_features: bad n");
     const int threads = 256;
@@ -202,7 +202,7 @@ extern "C" fugal_status fugal_average_neighbor_features(const int32_t* col_indic
                                                         int64_t n, const float* features, float* averages,
                                                         fugal_stream_t stream_) {
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
-    if (col_indices == nullptr || row_pointers == nullptr || features == nullptr || averages == nullptr)
+    if (row_pointers == nullptr || features == nullptr || averages == nullptr)
         return fail(FUGAL_BAD_ARGUMENT, "fugal_average_neighbor_features: null argument");
     if (n <= 0 || n > INT_MAX - 1) return fail(FUGAL_BAD_SHAPE, "fugal_average_neighbor_features: bad n");
     const int blocks = static_cast<int>(std::min<int64_t>((n + 127) / 128, 16 * sm_count()));

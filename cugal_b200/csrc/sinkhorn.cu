@@ -67,7 +67,9 @@ struct SolveState {
     int main_final_it;
     int main_n_err;
     int polish_count;
-    int pad0;
+    int exact_next;  // 1: the next sweep reduces rows with the exact (two-barrier) path
+    float max_corr;  // max |log colsum| of the current sweep (as float bits, atomicMax)
+    int pad1;
     double threshold;
     double omega;
     double err_accum;
@@ -161,6 +163,57 @@ __host__ __device__ constexpr int header_bytes() {
     return ((kBarBytes + 2 * (THREADS / 32) * R * 4 + 2 * kMaxCluster * R * 8) + 127) / 128 * 128;
 }
 
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kLn2 = 0.6931471805599453f;
+// Largest |column correction| (nats) after which the next sweep uses the exact
+// (max-stabilised) row reduction instead of the previous row normaliser.
+constexpr float kFastPathLimit = 30.0f;
+
+// 2^x on the MUFU unit (PTX ex2.approx.ftz.f32).
+FUGAL_DEVICE float ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Sum (or max) of one value per lane, the same in every lane.  The sum is lane
+// 0's butterfly result broadcast: every warp that reduces the same inputs then
+// holds the bit-identical value, so decisions taken on it are CTA-uniform.
+FUGAL_DEVICE float lanes_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+FUGAL_DEVICE float lanes_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// One cluster-wide exchange of per-row (max, sum) pairs through distributed
+// shared memory.  `xuse` counts the exchanges done so far (the same on every
+// CTA of the cluster) and selects the double-buffered slot and phase.  Thread 0
+// writes this CTA's pairs into every peer and arrives on every peer's barrier;
+// returns false (on every thread) if the wait timed out.
+template <int R>
+__device__ __forceinline__ bool cluster_exchange(float2* xch, uint64_t* xbar, int C, int rank, int& xuse,
+                                                 const float* m, const float* sm, int* err) {
+    const int slot = xuse & 1;
+    const uint32_t parity = static_cast<uint32_t>((xuse >> 1) & 1);
+    ++xuse;
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < C; ++k) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                st_cluster_f32x2(map_to_rank(&xch[(slot * kMaxCluster + rank) * R + r], k), m[r], sm[r]);
+            mbar_arrive_cluster(map_to_rank(&xbar[slot], k));
+        }
+        ok = mbar_wait(&xbar[slot], parity, err);
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
 template <typename T, int THREADS, int R, bool ABSORB, typename TOUT>
 __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
     constexpr int V = Vec<T>::N;
@@ -169,8 +222,8 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* xbar = full + kMaxStages;
-    float* red_max = reinterpret_cast<float*>(smem + kBarBytes);
-    float* red_sum = red_max + WARPS * R;
+    float* red_max = reinterpret_cast<float*>(smem + kBarBytes);  // [WARPS][R]
+    float* red_sum = red_max + WARPS * R;                         // [WARPS][R]
     float2* xch = reinterpret_cast<float2*>(red_sum + WARPS * R);
     float* b_s = reinterpret_cast<float*>(smem + header_bytes<THREADS, R>());
     unsigned char* stage_base = reinterpret_cast<unsigned char*>(b_s + p.slice_w);
@@ -179,9 +232,9 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
     if (*reinterpret_cast<volatile int*>(&st->done)) return;  // uniform: written by an earlier kernel
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int C = (int)cluster_nctarank();
-    const int rank = (int)cluster_ctarank();
-    const int cid = (int)cluster_id_x();
+    const int C = static_cast<int>(cluster_nctarank());
+    const int rank = static_cast<int>(cluster_ctarank());
+    const int cid = static_cast<int>(cluster_id_x());
     const int n = p.n;
     const int col0 = rank * p.slice_w;
     const int ncopy = max(0, min(p.slice_w, p.n_copy - col0));
@@ -191,7 +244,8 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
     const int nbatch = row_end > row_begin ? (row_end - row_begin + R - 1) / R : 0;
     const int t = st->it;
     const float omega = static_cast<float>(st->omega);
-    const bool momentum = fabsf(omega - 1.0f) > 0.0f;
+    const bool momentum = omega != 1.0f;
+    const bool exact_only = st->exact_next != 0 || momentum;  // uniform
     const uint32_t row_bytes = static_cast<uint32_t>(ncopy) * sizeof(T);
     const size_t stage_bytes = static_cast<size_t>(R) * p.slice_w * sizeof(T);
     const float* b_prev = p.b_buf + ((t - 1) & 1) * p.n_pad;
@@ -242,13 +296,22 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
         issued = min(p.stages, nbatch);
         for (int bt = 0; bt < issued; ++bt) issue(bt);
     }
+    auto release = [&](int bt) {  // stage of batch bt is free: refill it (thread 0)
+        if (tid == 0 && bt + p.stages < nbatch) {
+            fence_proxy_async_smem();
+            issue(bt + p.stages);
+            ++issued;
+        }
+    };
 
     float acc[kKPT];
 #pragma unroll
     for (int k = 0; k < kKPT; ++k) acc[k] = 0.f;
 
+    int xuse = 0;
+    bool alive = true;
     int bt = 0;
-    for (; bt < nbatch; ++bt) {
+    for (; bt < nbatch && alive; ++bt) {
         const int s = bt % p.stages;
         const bool okw = mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status);
         const int r0 = row_begin + bt * R;
@@ -256,121 +319,190 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
         const T* stage = reinterpret_cast<const T*>(stage_base + s * stage_bytes);
 
         float e[R][kKPT];
-        float mx[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) mx[r] = -INFINITY;
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-            const int c = (g * THREADS + tid) * V;
-            float bv[V];
-#pragma unroll
-            for (int q = 0; q < V; q += 4) {
-                const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + q);
-                bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (r < rows) {
-                    const uint4 raw = *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
-                    float vals[V];
-                    Vec<T>::unpack(raw, vals);
-#pragma unroll
-                    for (int q = 0; q < V; ++q) {
-                        const float x = (c + q < nvalid) ? vals[q] + bv[q] : -INFINITY;
-                        e[r][g * V + q] = x;
-                        mx[r] = fmaxf(mx[r], x);
-                    }
-                } else {
-#pragma unroll
-                    for (int q = 0; q < V; ++q) e[r][g * V + q] = -INFINITY;
-                }
-            }
-        }
+        float anew[R], wr[R];
         float a_old[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             a_old[r] = 0.f;
-            if (momentum && r < rows) {
+            if (r < rows) {
                 a_old[r] = p.a[r0 + r];
                 if (p.a_off != nullptr) a_old[r] += p.a_off[r0 + r];
             }
-            mx[r] = warp_max(mx[r]);
         }
-        if (lane == 0) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) red_max[warp * R + r] = mx[r];
-        }
-        if (!__syncthreads_and(okw)) break;  // S1: stage s fully read into registers
-        if (!ABSORB && tid == 0 && bt + p.stages < nbatch) {
-            fence_proxy_async_smem();
-            issue(bt + p.stages);
-            ++issued;
-        }
-        float Mc[R], sm[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            float m = -INFINITY;
-#pragma unroll
-            for (int w = 0; w < WARPS; ++w) m = fmaxf(m, red_max[w * R + r]);
-            Mc[r] = m;
-            const float base = (m == -INFINITY) ? 0.f : m;
-            float ssum = 0.f;
-#pragma unroll
-            for (int k = 0; k < kKPT; ++k) {
-                const float y = fast_exp(e[r][k] - base);
-                e[r][k] = y;
-                ssum += y;
-            }
-            sm[r] = warp_sum(ssum);
-        }
-        if (lane == 0) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) red_sum[warp * R + r] = sm[r];
-        }
-        __syncthreads();  // S2
-        float M[R], S[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            float ssum = 0.f;
-#pragma unroll
-            for (int w = 0; w < WARPS; ++w) ssum += red_sum[w * R + r];
-            M[r] = Mc[r];
-            S[r] = ssum;
-        }
-        if (C > 1) {
-            const int slot = bt & 1;
-            bool okx = true;
-            if (tid == 0) {
-                for (int k = 0; k < C; ++k) {
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        st_cluster_f32x2(map_to_rank(&xch[(slot * kMaxCluster + rank) * R + r], k), Mc[r], S[r]);
-                    mbar_arrive_cluster(map_to_rank(&xbar[slot], k));
-                }
-                okx = mbar_wait(&xbar[slot], static_cast<uint32_t>((bt >> 1) & 1), &st->status);
-            }
-            if (!__syncthreads_and(okx)) break;
+        bool fast_ok = false;
+        if (!exact_only) {
+            // ---- fast path: exponents relative to the previous row normaliser M_ref = -a_old
+            float mref2[R], sm[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                float m = -INFINITY;
-                for (int k = 0; k < C; ++k) m = fmaxf(m, xch[(slot * kMaxCluster + k) * R + r].x);
-                float ssum = 0.f;
-                for (int k = 0; k < C; ++k) {
-                    const float2 ps = xch[(slot * kMaxCluster + k) * R + r];
-                    if (ps.x != -INFINITY) ssum += ps.y * fast_exp(ps.x - m);
+                mref2[r] = -a_old[r] * kLog2e;
+                sm[r] = 0.f;
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int c = (g * THREADS + tid) * V;
+                float bv[V];
+#pragma unroll
+                for (int q = 0; q < V; q += 4) {
+                    const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + q);
+                    bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
                 }
-                M[r] = m;
-                S[r] = ssum;
+                const bool whole = c + V <= nvalid;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (r < rows) {
+                        const uint4 raw =
+                            *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
+                        float vals[V];
+                        Vec<T>::unpack(raw, vals);
+#pragma unroll
+                        for (int q = 0; q < V; ++q) {
+                            float y = ex2(fmaf(vals[q] + bv[q], kLog2e, -mref2[r]));
+                            if (!whole && c + q >= nvalid) y = 0.f;
+                            e[r][g * V + q] = y;
+                            sm[r] += y;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) sm[r] = warp_sum(sm[r]);
+            if (lane == 0) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) red_sum[warp * R + r] = sm[r];
+            }
+            if (!__syncthreads_and(okw)) {
+                alive = false;
+                break;
+            }
+            float S[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) S[r] = lanes_sum(lane < WARPS ? red_sum[lane * R + r] : 0.f);
+            if (C > 1) {
+                float zero[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) zero[r] = 0.f;
+                if (!cluster_exchange<R>(xch, xbar, C, rank, xuse, zero, S, &st->status)) {
+                    alive = false;
+                    break;
+                }
+                const int slot = (xuse - 1) & 1;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    float tot = 0.f;
+                    for (int k = 0; k < C; ++k) tot += xch[(slot * kMaxCluster + k) * R + r].y;
+                    S[r] = tot;
+                }
+            }
+            fast_ok = true;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r < rows && !(S[r] > 1e-30f && S[r] < 1e30f)) fast_ok = false;  // uniform
+            if (fast_ok) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    anew[r] = a_old[r] - logf(S[r]);  // -(M_ref + log S)
+                    wr[r] = 1.0f / S[r];
+                }
             }
         }
-        // Row update and the scale that turns e into the plan: P_ij = e_ij * w_r.
-        float anew[R], wr[R];
+        if (!fast_ok) {
+            // ---- exact path: CTA / cluster maximum first, then the exponentials
+            float mx[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const float lse = M[r] + logf(S[r]);
-            anew[r] = momentum ? (1.f - omega) * a_old[r] - omega * lse : -lse;
-            wr[r] = (Mc[r] == -INFINITY) ? 0.f : fast_exp(Mc[r] + anew[r]);
+            for (int r = 0; r < R; ++r) mx[r] = -INFINITY;
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int c = (g * THREADS + tid) * V;
+                float bv[V];
+#pragma unroll
+                for (int q = 0; q < V; q += 4) {
+                    const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + q);
+                    bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (r < rows) {
+                        const uint4 raw =
+                            *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
+                        float vals[V];
+                        Vec<T>::unpack(raw, vals);
+#pragma unroll
+                        for (int q = 0; q < V; ++q) {
+                            const float x = (c + q < nvalid) ? vals[q] + bv[q] : -INFINITY;
+                            e[r][g * V + q] = x;
+                            mx[r] = fmaxf(mx[r], x);
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < V; ++q) e[r][g * V + q] = -INFINITY;
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) mx[r] = warp_max(mx[r]);
+            if (lane == 0) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) red_max[warp * R + r] = mx[r];
+            }
+            if (!__syncthreads_and(okw)) {
+                alive = false;
+                break;
+            }
+            float Mc[R], Mc2[R], sm[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                Mc[r] = lanes_max(lane < WARPS ? red_max[lane * R + r] : -INFINITY);
+                Mc2[r] = (Mc[r] == -INFINITY) ? 0.f : Mc[r] * kLog2e;
+                float ssum = 0.f;
+#pragma unroll
+                for (int k = 0; k < kKPT; ++k) {
+                    const float y = ex2(fmaf(e[r][k], kLog2e, -Mc2[r]));
+                    e[r][k] = y;
+                    ssum += y;
+                }
+                sm[r] = warp_sum(ssum);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) red_sum[warp * R + r] = sm[r];
+            }
+            __syncthreads();
+            float M[R], S[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                S[r] = lanes_sum(lane < WARPS ? red_sum[lane * R + r] : 0.f);
+                M[r] = Mc[r];
+            }
+            if (C > 1) {
+                if (!cluster_exchange<R>(xch, xbar, C, rank, xuse, Mc, S, &st->status)) {
+                    alive = false;
+                    break;
+                }
+                const int slot = (xuse - 1) & 1;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    float m = -INFINITY;
+                    for (int k = 0; k < C; ++k) m = fmaxf(m, xch[(slot * kMaxCluster + k) * R + r].x);
+                    float ssum = 0.f;
+                    for (int k = 0; k < C; ++k) {
+                        const float2 ps = xch[(slot * kMaxCluster + k) * R + r];
+                        if (ps.x != -INFINITY) ssum += ps.y * ex2((ps.x - m) * kLog2e);
+                    }
+                    M[r] = m;
+                    S[r] = ssum;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const float lse = M[r] + logf(S[r]);
+                anew[r] = momentum ? (1.f - omega) * a_old[r] - omega * lse : -lse;
+                wr[r] = (Mc[r] == -INFINITY) ? 0.f : ex2((Mc[r] + anew[r]) * kLog2e);
+            }
         }
+        // Stage s is no longer read by the row reduction; the absorb variant
+        // still re-reads it below.
+        if (!ABSORB) release(bt);
         if (rank == 0 && tid < rows) {
             float v = anew[0];
 #pragma unroll
@@ -383,6 +515,7 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
                 p.a[r0 + tid] = v;
             }
         }
+        // Column sums of the row-normalised plan P_ij = e_ij * w_r.
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (r < rows) {
@@ -416,11 +549,7 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
                 }
             }
             __syncthreads();
-            if (tid == 0 && bt + p.stages < nbatch) {
-                fence_proxy_async_smem();
-                issue(bt + p.stages);
-                ++issued;
-            }
+            release(bt);
         }
     }
 
@@ -429,14 +558,21 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
 #pragma unroll
     for (int g = 0; g < G; ++g) {
         const int c = (g * THREADS + tid) * V;
+        if (c + V <= nvalid) {
 #pragma unroll
-        for (int q = 0; q < V; ++q)
-            if (c + q < nvalid) prow[c + q] = acc[g * V + q];
+            for (int q = 0; q < V; q += 4)
+                *reinterpret_cast<float4*>(prow + c + q) =
+                    make_float4(acc[g * V + q], acc[g * V + q + 1], acc[g * V + q + 2], acc[g * V + q + 3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < V; ++q)
+                if (c + q < nvalid) prow[c + q] = acc[g * V + q];
+        }
     }
 
     // An early exit (timed-out wait) may leave bulk copies in flight: wait for
     // them, again bounded, before the shared memory goes away.
-    if (bt < nbatch && tid == 0) {
+    if (!alive && tid == 0) {
         for (int b = bt; b < issued; ++b)
             if (!mbar_wait(&full[b % p.stages], static_cast<uint32_t>((b / p.stages) & 1), &st->status)) break;
     }
@@ -444,28 +580,65 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
 }
 
 // Reduce the per-cluster column sums (FP64), write log(colsum), decide.
-__global__ void finalize_kernel(const float* partials, int nparts, long long n_pad, int n, float* logcs,
-                                SolveState* st) {
+// Block: 8 warps x 32 lanes; lanes own 4 consecutive columns each (128 per
+// block), warps split the partial rows; one FP64 error sum and one maximum
+// |column correction| per block go to the solve state by atomics.
+constexpr int kFinThreads = 256;
+constexpr int kFinCols = 128;
+
+__global__ void __launch_bounds__(kFinThreads) finalize_kernel(const float* partials, int nparts, long long n_pad,
+                                                               int n, float* logcs, SolveState* st) {
+    __shared__ double part[kFinThreads / 32][kFinCols];
     __shared__ double red[32];
+    __shared__ float red_corr[kFinThreads / 32];
     if (*reinterpret_cast<volatile int*>(&st->done)) return;
-    double err = 0.0;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        double cs = 0.0;
-        for (int c = 0; c < nparts; ++c) cs += static_cast<double>(partials[static_cast<size_t>(c) * n_pad + j]);
-        err += fabs(cs - 1.0);
-        logcs[j] = static_cast<float>(log(fmax(cs, 1e-37)));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j0 = blockIdx.x * kFinCols + lane * 4;
+    double cs[4] = {0.0, 0.0, 0.0, 0.0};
+    if (j0 < n) {
+        for (int c = warp; c < nparts; c += kFinThreads / 32) {
+            const float4 v = *reinterpret_cast<const float4*>(partials + static_cast<size_t>(c) * n_pad + j0);
+            cs[0] += v.x; cs[1] += v.y; cs[2] += v.z; cs[3] += v.w;
+        }
     }
-    err = block_sum(err, red);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) part[warp][lane * 4 + q] = cs[q];
+    __syncthreads();
+    double err = 0.0;
+    float corr = 0.f;
+    if (threadIdx.x < kFinCols) {
+        const int j = blockIdx.x * kFinCols + threadIdx.x;
+        if (j < n) {
+            double tot = 0.0;
+#pragma unroll
+            for (int w = 0; w < kFinThreads / 32; ++w) tot += part[w][threadIdx.x];
+            err = fabs(tot - 1.0);
+            const float lg = static_cast<float>(log(fmax(tot, 1e-37)));
+            logcs[j] = lg;
+            corr = fabsf(lg);
+        }
+    }
+    corr = warp_max(corr);
+    if (lane == 0) red_corr[warp] = corr;
+    err = block_sum(err, red);  // contains __syncthreads: red_corr is complete
     if (threadIdx.x == 0) {
+        float bc = 0.f;
+        for (int w = 0; w < kFinThreads / 32; ++w) bc = fmaxf(bc, red_corr[w]);
+        if (bc > 0.f) atomicMax(reinterpret_cast<unsigned int*>(&st->max_corr), __float_as_uint(bc));
         atomicAdd(&st->err_accum, err);
         __threadfence();
         const unsigned prev = atomicAdd(&st->ticket, 1u);
         if (prev == gridDim.x - 1) {
             __threadfence();
             const double total = atomicAdd(&st->err_accum, 0.0);
+            const float max_corr = __uint_as_float(atomicOr(reinterpret_cast<unsigned int*>(&st->max_corr), 0u));
             st->err_accum = 0.0;
             st->ticket = 0;
+            st->max_corr = 0.f;
             decide(st, total);
+            // the next sweep may use the previous row normaliser as its reference
+            // only if no column moves by more than kFastPathLimit nats
+            st->exact_next = (max_corr * static_cast<float>(st->omega) > kFastPathLimit || st->omega != 1.0) ? 1 : 0;
         }
     }
 }
@@ -548,6 +721,8 @@ __global__ void column_merge_kernel(const float2* part, int nchunks, long long n
         st->main_final_it = -1;
         st->main_n_err = 0;
         st->polish_count = 0;
+        st->exact_next = 1;
+        st->max_corr = 0.f;
         st->threshold = ia.threshold;
         st->omega = 1.0;
         st->err_accum = 0.0;
@@ -601,6 +776,7 @@ __global__ void polish_begin_kernel(SolveState* st, float* a, float* b_buf, long
         st->max_it = fin + 1 + f.polish;
         st->check = 0;
         st->omega = 1.0;
+        st->exact_next = 1;
     }
 }
 
@@ -934,10 +1110,11 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         a.st = w.st;
         return a;
     };
+    const int fin_grid = static_cast<int>((n + kFinCols - 1) / kFinCols);
     auto finalize = [&](int nparts) -> fugal_status {
         LaunchScope scope(FUGAL_KERNEL_FINALIZE, stream);
-        finalize_kernel<<<fin_blocks, 256, 0, stream>>>(w.partials, nparts, w.n_pad, static_cast<int>(n), w.logcs,
-                                                        w.st);
+        finalize_kernel<<<fin_grid, kFinThreads, 0, stream>>>(w.partials, nparts, w.n_pad, static_cast<int>(n),
+                                                              w.logcs, w.st);
         return launch_check("sinkhorn: finalize");
     };
 

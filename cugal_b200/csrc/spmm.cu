@@ -31,9 +31,24 @@ constexpr int kTileRows = 32;     // gathered output rows per CTA
 constexpr int kTileCols = 128;    // columns per CTA (32 lanes x float4)
 constexpr int kSpmmThreads = 256; // 8 warps, 4 rows each
 
-// acc = sum over k in N(row) of X[k][c0 .. c0+3] (float4 per lane).
+// 4 consecutive floats of row k starting at column c: one 16-byte load when the
+// rows are 16-byte aligned (VEC), else scalar loads guarded by n.
+template <bool VEC>
+__device__ __forceinline__ float4 load4(const float* __restrict__ X, long long ldx, int k, int c, int n) {
+    const float* p = X + static_cast<size_t>(k) * ldx + c;
+    if (VEC) return __ldg(reinterpret_cast<const float4*>(p));
+    float4 v;
+    v.x = __ldg(p);
+    v.y = c + 1 < n ? __ldg(p + 1) : 0.f;
+    v.z = c + 2 < n ? __ldg(p + 2) : 0.f;
+    v.w = c + 3 < n ? __ldg(p + 3) : 0.f;
+    return v;
+}
+
+// acc = sum over k in N(row) of X[k][c .. c+3] (4 columns per lane).
+template <bool VEC>
 __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const int* __restrict__ col,
-                                             const float* __restrict__ X, long long ldx, int row, int c,
+                                             const float* __restrict__ X, long long ldx, int n, int row, int c,
                                              bool c_ok) {
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     const int lane = threadIdx.x & 31;
@@ -48,10 +63,10 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
             const int k2 = __shfl_sync(0xffffffffu, idx, q + 2);
             const int k3 = __shfl_sync(0xffffffffu, idx, q + 3);
             if (c_ok) {
-                const float4 v0 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k0) * ldx + c));
-                const float4 v1 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k1) * ldx + c));
-                const float4 v2 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k2) * ldx + c));
-                const float4 v3 = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k3) * ldx + c));
+                const float4 v0 = load4<VEC>(X, ldx, k0, c, n);
+                const float4 v1 = load4<VEC>(X, ldx, k1, c, n);
+                const float4 v2 = load4<VEC>(X, ldx, k2, c, n);
+                const float4 v3 = load4<VEC>(X, ldx, k3, c, n);
                 acc.x += v0.x; acc.y += v0.y; acc.z += v0.z; acc.w += v0.w;
                 acc.x += v1.x; acc.y += v1.y; acc.z += v1.z; acc.w += v1.w;
                 acc.x += v2.x; acc.y += v2.y; acc.z += v2.z; acc.w += v2.w;
@@ -61,7 +76,7 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
         for (; q < cnt; ++q) {
             const int k = __shfl_sync(0xffffffffu, idx, q);
             if (c_ok) {
-                const float4 v = __ldg(reinterpret_cast<const float4*>(X + static_cast<size_t>(k) * ldx + c));
+                const float4 v = load4<VEC>(X, ldx, k, c, n);
                 acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
             }
         }
@@ -70,6 +85,7 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
 }
 
 // Fill tile[r][0..127] with the gathered rows r0 .. r0+31 of A X for columns c0 .. c0+127.
+template <bool VEC>
 __device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const int* __restrict__ col,
                                             const float* __restrict__ X, long long ldx, int n, int r0, int c0,
                                             float (*tile)[kTileCols + 1], float sign) {
@@ -79,7 +95,7 @@ __device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const in
     for (int rr = warp; rr < kTileRows; rr += kSpmmThreads / 32) {
         const int row = r0 + rr;
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row < n) acc = gather_row(rp, col, X, ldx, row, c, c_ok);
+        if (row < n) acc = gather_row<VEC>(rp, col, X, ldx, n, row, c, c_ok);
         tile[rr][lane * 4 + 0] = sign * acc.x;
         tile[rr][lane * 4 + 1] = sign * acc.y;
         tile[rr][lane * 4 + 2] = sign * acc.z;
@@ -88,6 +104,7 @@ __device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const in
 }
 
 // Tt[c][r] = (A X)[r][c]  (transposed store), or out[r][c] = sign (A X)[r][c] (direct store).
+template <bool VEC>
 __global__ void __launch_bounds__(kSpmmThreads) spmm_kernel(const int* __restrict__ rp, const int* __restrict__ col,
                                                             const float* __restrict__ X, long long ldx, int n,
                                                             float* __restrict__ out, long long ldo, int transpose,
@@ -95,7 +112,7 @@ __global__ void __launch_bounds__(kSpmmThreads) spmm_kernel(const int* __restric
     __shared__ float tile[kTileRows][kTileCols + 1];
     const int r0 = blockIdx.x * kTileRows;
     const int c0 = blockIdx.y * kTileCols;
-    gather_tile(rp, col, X, ldx, n, r0, c0, tile, sign);
+    gather_tile<VEC>(rp, col, X, ldx, n, r0, c0, tile, sign);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (transpose) {
@@ -149,7 +166,7 @@ __global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __res
         for (int q = threadIdx.x; q < kTileRows; q += kSpmmThreads)
             fj[q] = (j0 + q < n) ? reinterpret_cast<const float4*>(ep.ft)[j0 + q] : make_float4(0, 0, 0, 0);
     }
-    gather_tile(rp, col, Tt, ldt, n, j0, i0, tile, 1.0f);
+    gather_tile<true>(rp, col, Tt, ldt, n, j0, i0, tile, 1.0f);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = j0 + lane;
@@ -188,8 +205,10 @@ __global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const
     outT[static_cast<size_t>(j) * ldo + i] = sign * acc;
 }
 
+// col may be null for a graph without edges (it is never dereferenced then).
 fugal_status check_csr(const int32_t* rp, const int32_t* col, int64_t n, const char* who) {
-    if (rp == nullptr || col == nullptr) return fail(FUGAL_BAD_ARGUMENT, "%s: null CSR pointer", who);
+    (void)col;
+    if (rp == nullptr) return fail(FUGAL_BAD_ARGUMENT, "%s: null row pointers", who);
     if (n <= 0 || n > (1ll << 30)) return fail(FUGAL_BAD_SHAPE, "%s: bad n", who);
     return FUGAL_OK;
 }
@@ -208,12 +227,14 @@ extern "C" fugal_status fugal_adjacency_matmul(const int32_t* col_indices, const
     const float sign = negate ? -1.f : 1.f;
     LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
     if (!m_transposed) {
-        if ((ldm % 4) != 0 || !aligned16(M))
-            return fail(FUGAL_BAD_SHAPE, "fugal_adjacency_matmul: M needs ld %% 4 == 0 and a 16-byte base");
         dim3 grid(static_cast<unsigned>((n + kTileRows - 1) / kTileRows),
                   static_cast<unsigned>((n + kTileCols - 1) / kTileCols));
-        spmm_kernel<<<grid, kSpmmThreads, 0, stream>>>(row_pointers, col_indices, M, ldm, static_cast<int>(n), out,
-                                                        ldo, 0, sign);
+        if ((ldm % 4) == 0 && aligned16(M))
+            spmm_kernel<true><<<grid, kSpmmThreads, 0, stream>>>(row_pointers, col_indices, M, ldm,
+                                                                  static_cast<int>(n), out, ldo, 0, sign);
+        else
+            spmm_kernel<false><<<grid, kSpmmThreads, 0, stream>>>(row_pointers, col_indices, M, ldm,
+                                                                   static_cast<int>(n), out, ldo, 0, sign);
     } else {
         dim3 grid(static_cast<unsigned>(n), static_cast<unsigned>((n + 127) / 128));
         spmm_transposed_operand_kernel<<<grid, 128, 0, stream>>>(row_pointers, col_indices, M, ldm,
@@ -262,8 +283,8 @@ extern "C" fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointe
               static_cast<unsigned>((n + kTileCols - 1) / kTileCols));
     {
         LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
-        spmm_kernel<<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp, static_cast<int>(n), Tt,
-                                                        ldt, 1, 1.f);
+        spmm_kernel<true><<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp,
+                                                              static_cast<int>(n), Tt, ldt, 1, 1.f);
         FUGAL_TRY(launch_check("fugal_fw_gradient: A P"));
     }
     EpilogueArgs ep{P, ldp, source_features, target_features, D, ldd, lambda * lambda_scale, out_scale, U, V, out,

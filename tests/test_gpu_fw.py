@@ -96,13 +96,16 @@ def test_sinkhorn_fp32_matches_oracle(n, slice_w, monkeypatch):
     C = C.astype(np.float32).astype(np.float64)
     reg, freq = 0.05, 10
     max_iter = 30 if n >= 5000 else (60 if n >= 3000 else 200)
-    thr = 1e-9 if n >= 3000 else 5e-5
+    # FP32 cannot push the summed column error below ~n * 1e-7; thresholds sit above that floor
+    thr = 0.0 if n >= 3000 else 1e-3
     zero = np.zeros(n)
     ref = O.sinkhorn_log_solve(C, zero, zero, reg, max_iter, thr, freq)
     u, v, prof = _solve_gpu(C, zero, zero, reg, max_iter, thr, freq)
     assert abs(prof.iteration_count - ref.iteration_count) <= freq
     if ref.iteration_count < max_iter and min(abs(np.array(ref.errors) / thr - 1)) > 0.2:
         assert prof.iteration_count == ref.iteration_count
+    k = min(len(prof.errors), len(ref.errors))
+    np.testing.assert_allclose(prof.errors[:k], ref.errors[:k], rtol=2e-2, atol=5e-7 * n)
     # the two solutions share the same gauge (same iteration), compare duals and plans
     np.testing.assert_allclose(u, ref.u, atol=2e-4 * max(1.0, np.abs(ref.u).max() / 100))
     np.testing.assert_allclose(v, ref.v, atol=2e-4 * max(1.0, np.abs(ref.v).max() / 100))
@@ -132,10 +135,11 @@ def test_sinkhorn_momentum_matches_oracle():
     rng = np.random.default_rng(5)
     C = (rng.random((n, n)) * 4).astype(np.float32).astype(np.float64)
     zero = np.zeros(n)
-    ref = O.sinkhorn_log_solve(C, zero, zero, 0.05, 300, 1e-7, 5, momentum_start=10)
-    u, v, prof = _solve_gpu(C, zero, zero, 0.05, 300, 1e-7, 5, mstart=10)
-    assert abs(prof.iteration_count - ref.iteration_count) <= 5
-    np.testing.assert_allclose(prof.errors[:3], ref.errors[:3], rtol=1e-3)
+    # threshold above the FP32 floor (~n * 5e-8) so both stop on the same evaluation
+    ref = O.sinkhorn_log_solve(C, zero, zero, 0.05, 300, 1e-4, 5, momentum_start=10)
+    u, v, prof = _solve_gpu(C, zero, zero, 0.05, 300, 1e-4, 5, mstart=10)
+    assert prof.iteration_count == ref.iteration_count
+    np.testing.assert_allclose(prof.errors, ref.errors, rtol=2e-2)
     np.testing.assert_allclose(_plan(C, u, v, 0.05), _plan(C, ref.u, ref.v, 0.05), atol=2e-4)
 
 
@@ -244,6 +248,8 @@ def test_full_alignment_matches_oracle(lap):
     assert max(abs(a - b) for a, b in zip(its, trace.sinkhorn_iterations)) <= 10
     assert [m[1] for m in mapping] == [m[1] for m in mref]
     np.testing.assert_allclose(P, Pr, atol=2e-3)
-    assert abs(prof.sparsity - sp) < 0.02
+    # the reference's GPU path counts entries <= FP32 epsilon (its P is FP32)
+    sp32 = float(np.sum(Pr <= np.finfo(np.float32).eps)) / Pr.size
+    assert abs(prof.sparsity - sp32) < 0.02
     from cugal_b200 import Phase
     assert set(prof.phase_times) == set(Phase)
