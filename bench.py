@@ -313,6 +313,7 @@ def run_ours(args):
     e2e_acc = node_accuracy(mapping, perm) if e2e_times else None
 
     ld = padded_ld(n)
+    plan = N.sinkhorn_plan(n, N.STREAM_DTYPES[sdt])
     peak, peak_kind = load_peak()
     fam_key = "sweep16" if sdt is not None else "sweep32"
     nl, ms = fam[fam_key]
@@ -355,7 +356,7 @@ def run_ours(args):
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "kernel": f"sweep_kernel<{args.stream_dtype}>", "launches": nl,
                          "avg_launch_ms": ms / nl if nl else None, "bytes_per_launch": bytes_per,
-                         "peak_kind": peak_kind},
+                         "peak_kind": peak_kind, "launch_shape": plan},
             "kernel_times_ms": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in fam.items()},
             "cpu_baseline": cpu,
             "reference_gpu_fp32": ref_gpu,

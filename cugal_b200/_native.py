@@ -74,6 +74,7 @@ SIGNATURES = {
     "fugal_fw_gradient": (_INT, [_I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _I64, _D, _D, _D, _P, _P, _P, _I64,
                                  _P, _SZ, _P]),
     "fugal_sinkhorn_workspace_size": (_INT, [_I64, _INT, POINTER(c_size_t)]),
+    "fugal_sinkhorn_plan_info": (_INT, [_I64, _INT, _P]),
     "fugal_sinkhorn_solve": (_INT, [POINTER(SolveParams), _P, _SZ, _P]),
     "fugal_fw_update": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _P]),
     "fugal_timing_enable": (None, [_INT]),
@@ -151,6 +152,14 @@ def timing_query(family: int) -> tuple[int, float]:
     n, ms = c_int64(0), c_double(0.0)
     call("fugal_timing_query", family, ctypes.byref(n), ctypes.byref(ms))
     return n.value, ms.value
+
+
+def sinkhorn_plan(n: int, stream_dtype: int) -> dict:
+    """Launch shape the solve uses for size n on the current device."""
+    info = (ctypes.c_int32 * 6)()
+    call("fugal_sinkhorn_plan_info", n, stream_dtype, ctypes.cast(info, c_void_p))
+    keys = ["threads", "cluster", "clusters", "stages", "smem_bytes", "rows_per_batch"]
+    return dict(zip(keys, list(info)))
 
 
 def launch_count() -> int:

@@ -198,6 +198,19 @@ FUGAL_DEVICE uint32_t map_to_rank(const void* p, uint32_t rank) {
 FUGAL_DEVICE void st_cluster_f32x2(uint32_t addr, float a, float b) {
     asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(a), "f"(b) : "memory");
 }
+// Asynchronous store of two floats into (possibly another CTA's) shared memory
+// that completes 8 bytes of transaction count on that CTA's mbarrier.
+FUGAL_DEVICE void st_async_f32x2(uint32_t remote_addr, float a, float b, uint32_t remote_bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f32 [%0], {%1, %2}, [%3];" ::"r"(
+                     remote_addr),
+                 "f"(a), "f"(b), "r"(remote_bar)
+                 : "memory");
+}
+// Cluster-wide barrier that tolerates divergent threads (no .aligned).
+FUGAL_DEVICE void cluster_sync_any() {
+    asm volatile("barrier.cluster.arrive.release;\n"
+                 "barrier.cluster.wait.acquire;" ::: "memory");
+}
 FUGAL_DEVICE void mbar_arrive_cluster(uint32_t remote_bar_addr) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote_bar_addr)
                  : "memory");

@@ -157,12 +157,6 @@ struct SweepArgs {
 
 constexpr int kBarBytes = 128;
 
-template <int THREADS, int R>
-__host__ __device__ constexpr int header_bytes() {
-    // barriers + red_max/red_sum [WARPS][R] + xch [2][kMaxCluster][R] float2, rounded to 128
-    return ((kBarBytes + 2 * (THREADS / 32) * R * 4 + 2 * kMaxCluster * R * 8) + 127) / 128 * 128;
-}
-
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kLn2 = 0.6931471805599453f;
 // Largest |column correction| (nats) after which the next sweep uses the exact
@@ -190,48 +184,78 @@ FUGAL_DEVICE float lanes_max(float v) {
     return v;
 }
 
-// One cluster-wide exchange of per-row (max, sum) pairs through distributed
-// shared memory.  `xuse` counts the exchanges done so far (the same on every
-// CTA of the cluster) and selects the double-buffered slot and phase.  Thread 0
-// writes this CTA's pairs into every peer and arrives on every peer's barrier;
-// returns false (on every thread) if the wait timed out.
-template <int R>
-__device__ __forceinline__ bool cluster_exchange(float2* xch, uint64_t* xbar, int C, int rank, int& xuse,
-                                                 const float* m, const float* sm, int* err) {
+// Shared-memory layout of the sweep kernel (byte offsets from the dynamic base):
+//   [0, 128)          mbarriers: full[kMaxStages] (stage loaded), xbar[2] (exchange done)
+//   [128, header)     xch[2][kMaxCluster][WARPS][R] float2: per-warp row partials of every CTA
+//   [header, +4 W)    b_s[slice_w]: this sweep's column duals for the CTA's slice
+//   then              stages[stages][R][slice_w] elements of the streamed cost
+template <int THREADS, int R>
+__host__ __device__ constexpr int header_bytes_v3() {
+    return ((kBarBytes + 2 * kMaxCluster * (THREADS / 32) * R * 8) + 127) / 128 * 128;
+}
+
+// One cluster-wide all-to-all of per-warp row partials.  Every warp sends its R
+// (max, sum) pairs into every CTA of the cluster with st.async (lanes 0..C-1 in
+// parallel, one peer each), completing transaction bytes on the receiver's
+// exchange barrier; thread 0 arms its own barrier with the bytes it expects.
+// `xuse` counts exchanges (identical on every CTA) and selects slot and phase.
+// Returns the slot to read, or -1 if the wait timed out.
+template <int THREADS, int R>
+__device__ __forceinline__ int exchange(float2* xch, uint64_t* xbar, int C, int rank, int& xuse, const float* m,
+                                        const float* sm, int* err) {
+    constexpr int WARPS = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int slot = xuse & 1;
     const uint32_t parity = static_cast<uint32_t>((xuse >> 1) & 1);
     ++xuse;
-    bool ok = true;
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < C; ++k) {
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&xbar[slot], static_cast<uint32_t>(C * WARPS * R * 8));
+    if (lane < C) {
+        const uint32_t bar = map_to_rank(&xbar[slot], lane);
 #pragma unroll
-            for (int r = 0; r < R; ++r)
-                st_cluster_f32x2(map_to_rank(&xch[(slot * kMaxCluster + rank) * R + r], k), m[r], sm[r]);
-            mbar_arrive_cluster(map_to_rank(&xbar[slot], k));
-        }
-        ok = mbar_wait(&xbar[slot], parity, err);
+        for (int r = 0; r < R; ++r)
+            st_async_f32x2(map_to_rank(&xch[((slot * kMaxCluster + rank) * WARPS + warp) * R + r], lane), m[r], sm[r],
+                           bar);
     }
-    return __syncthreads_and(ok) != 0;
+    return mbar_wait(&xbar[slot], parity, err) ? slot : -1;
 }
 
+// Reductions over the C x WARPS partials of one row held in slot `slot`: every
+// lane reads a strided subset, then a butterfly; lane 0's result is broadcast so
+// every thread of every CTA holds the bit-identical value.
+template <int THREADS, int R>
+__device__ __forceinline__ float slot_max(const float2* xch, int slot, int C, int r) {
+    constexpr int WARPS = THREADS / 32;
+    const int lane = threadIdx.x & 31;
+    float v = -INFINITY;
+    for (int i = lane; i < C * WARPS; i += 32) v = fmaxf(v, xch[(slot * kMaxCluster * WARPS + i) * R + r].x);
+    return __shfl_sync(0xffffffffu, lanes_max(v), 0);
+}
+template <int THREADS, int R>
+__device__ __forceinline__ float slot_sum(const float2* xch, int slot, int C, int r) {
+    constexpr int WARPS = THREADS / 32;
+    const int lane = threadIdx.x & 31;
+    float v = 0.f;
+    for (int i = lane; i < C * WARPS; i += 32) v += xch[(slot * kMaxCluster * WARPS + i) * R + r].y;
+    return lanes_sum(v);
+}
+
+// At most 128 registers per thread so that 512 threads' worth of CTAs share an SM.
 template <typename T, int THREADS, int R, bool ABSORB, typename TOUT>
-__global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
+__global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS)) sweep_kernel(const SweepArgs p) {
     constexpr int V = Vec<T>::N;
     constexpr int G = kKPT / V;
-    constexpr int WARPS = THREADS / 32;
     extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int abort_s;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* xbar = full + kMaxStages;
-    float* red_max = reinterpret_cast<float*>(smem + kBarBytes);  // [WARPS][R]
-    float* red_sum = red_max + WARPS * R;                         // [WARPS][R]
-    float2* xch = reinterpret_cast<float2*>(red_sum + WARPS * R);
-    float* b_s = reinterpret_cast<float*>(smem + header_bytes<THREADS, R>());
+    float2* xch = reinterpret_cast<float2*>(smem + kBarBytes);
+    float* b_s = reinterpret_cast<float*>(smem + header_bytes_v3<THREADS, R>());
     unsigned char* stage_base = reinterpret_cast<unsigned char*>(b_s + p.slice_w);
 
     SolveState* st = p.st;
     if (*reinterpret_cast<volatile int*>(&st->done)) return;  // uniform: written by an earlier kernel
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int C = static_cast<int>(cluster_nctarank());
     const int rank = static_cast<int>(cluster_ctarank());
     const int cid = static_cast<int>(cluster_id_x());
@@ -271,12 +295,13 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
     }
     if (tid == 0) {
         for (int s = 0; s < p.stages; ++s) mbar_init(&full[s], 1);
-        mbar_init(&xbar[0], C);
-        mbar_init(&xbar[1], C);
+        mbar_init(&xbar[0], 1);
+        mbar_init(&xbar[1], 1);
         fence_mbarrier_init();
+        abort_s = 0;
     }
     __syncthreads();
-    if (C > 1) cluster_sync();  // every peer's barriers exist before the first remote arrive
+    cluster_sync();  // every peer's barriers exist before the first remote transaction
 
     auto issue = [&](int bt) {
         const int s = bt % p.stages;
@@ -296,12 +321,21 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
         issued = min(p.stages, nbatch);
         for (int bt = 0; bt < issued; ++bt) issue(bt);
     }
-    auto release = [&](int bt) {  // stage of batch bt is free: refill it (thread 0)
+    // Stage of batch bt is no longer read: refill it with batch bt + stages (thread 0).
+    auto release = [&](int bt) {
         if (tid == 0 && bt + p.stages < nbatch) {
             fence_proxy_async_smem();
             issue(bt + p.stages);
             ++issued;
         }
+    };
+    // Failure handling: a timed-out wait aborts the whole CTA.  The absorb
+    // variant (which has CTA barriers) agrees through __syncthreads_and; the
+    // others through a shared flag every thread checks after each wait.
+    auto agree = [&](bool ok) -> bool {
+        if (ABSORB) return __syncthreads_and(ok) != 0;
+        if (!ok) abort_s = 1;
+        return ok && *reinterpret_cast<volatile int*>(&abort_s) == 0;
     };
 
     float acc[kKPT];
@@ -311,16 +345,18 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
     int xuse = 0;
     bool alive = true;
     int bt = 0;
-    for (; bt < nbatch && alive; ++bt) {
+    for (; bt < nbatch; ++bt) {
         const int s = bt % p.stages;
-        const bool okw = mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status);
+        if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status))) {
+            alive = false;
+            break;
+        }
         const int r0 = row_begin + bt * R;
         const int rows = min(R, row_end - r0);
         const T* stage = reinterpret_cast<const T*>(stage_base + s * stage_bytes);
 
         float e[R][kKPT];
-        float anew[R], wr[R];
-        float a_old[R];
+        float anew[R], wr[R], a_old[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             a_old[r] = 0.f;
@@ -331,12 +367,13 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
         }
         bool fast_ok = false;
         if (!exact_only) {
-            // ---- fast path: exponents relative to the previous row normaliser M_ref = -a_old
-            float mref2[R], sm[R];
+            // ---- fast path: exponents relative to the previous row normaliser -a_old
+            float mref2[R], sm[R], zero[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 mref2[r] = -a_old[r] * kLog2e;
                 sm[r] = 0.f;
+                zero[r] = 0.f;
             }
 #pragma unroll
             for (int g = 0; g < G; ++g) {
@@ -367,50 +404,35 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) sm[r] = warp_sum(sm[r]);
-            if (lane == 0) {
-#pragma unroll
-                for (int r = 0; r < R; ++r) red_sum[warp * R + r] = sm[r];
-            }
-            if (!__syncthreads_and(okw)) {
+            const int slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status);
+            if (!agree(slot >= 0)) {
                 alive = false;
                 break;
             }
             float S[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) S[r] = lanes_sum(lane < WARPS ? red_sum[lane * R + r] : 0.f);
-            if (C > 1) {
-                float zero[R];
-#pragma unroll
-                for (int r = 0; r < R; ++r) zero[r] = 0.f;
-                if (!cluster_exchange<R>(xch, xbar, C, rank, xuse, zero, S, &st->status)) {
-                    alive = false;
-                    break;
-                }
-                const int slot = (xuse - 1) & 1;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    float tot = 0.f;
-                    for (int k = 0; k < C; ++k) tot += xch[(slot * kMaxCluster + k) * R + r].y;
-                    S[r] = tot;
-                }
-            }
             fast_ok = true;
 #pragma unroll
-            for (int r = 0; r < R; ++r)
+            for (int r = 0; r < R; ++r) {
+                S[r] = slot_sum<THREADS, R>(xch, slot, C, r);
                 if (r < rows && !(S[r] > 1e-30f && S[r] < 1e30f)) fast_ok = false;  // uniform
+            }
             if (fast_ok) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     anew[r] = a_old[r] - logf(S[r]);  // -(M_ref + log S)
                     wr[r] = 1.0f / S[r];
                 }
+                if (!ABSORB) release(bt);
             }
         }
         if (!fast_ok) {
-            // ---- exact path: CTA / cluster maximum first, then the exponentials
-            float mx[R];
+            // ---- exact path: cluster-wide row maximum first, then the exponentials
+            float mx[R], zero[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) mx[r] = -INFINITY;
+            for (int r = 0; r < R; ++r) {
+                mx[r] = -INFINITY;
+                zero[r] = 0.f;
+            }
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int c = (g * THREADS + tid) * V;
@@ -441,68 +463,39 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) mx[r] = warp_max(mx[r]);
-            if (lane == 0) {
-#pragma unroll
-                for (int r = 0; r < R; ++r) red_max[warp * R + r] = mx[r];
-            }
-            if (!__syncthreads_and(okw)) {
+            int slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, mx, zero, &st->status);
+            if (!agree(slot >= 0)) {
                 alive = false;
                 break;
             }
-            float Mc[R], Mc2[R], sm[R];
+            if (!ABSORB) release(bt);
+            float M[R], M2[R], sm[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                Mc[r] = lanes_max(lane < WARPS ? red_max[lane * R + r] : -INFINITY);
-                Mc2[r] = (Mc[r] == -INFINITY) ? 0.f : Mc[r] * kLog2e;
+                M[r] = slot_max<THREADS, R>(xch, slot, C, r);
+                M2[r] = (M[r] == -INFINITY) ? 0.f : M[r] * kLog2e;
                 float ssum = 0.f;
 #pragma unroll
                 for (int k = 0; k < kKPT; ++k) {
-                    const float y = ex2(fmaf(e[r][k], kLog2e, -Mc2[r]));
+                    const float y = ex2(fmaf(e[r][k], kLog2e, -M2[r]));
                     e[r][k] = y;
                     ssum += y;
                 }
                 sm[r] = warp_sum(ssum);
             }
-            if (lane == 0) {
-#pragma unroll
-                for (int r = 0; r < R; ++r) red_sum[warp * R + r] = sm[r];
-            }
-            __syncthreads();
-            float M[R], S[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                S[r] = lanes_sum(lane < WARPS ? red_sum[lane * R + r] : 0.f);
-                M[r] = Mc[r];
-            }
-            if (C > 1) {
-                if (!cluster_exchange<R>(xch, xbar, C, rank, xuse, Mc, S, &st->status)) {
-                    alive = false;
-                    break;
-                }
-                const int slot = (xuse - 1) & 1;
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    float m = -INFINITY;
-                    for (int k = 0; k < C; ++k) m = fmaxf(m, xch[(slot * kMaxCluster + k) * R + r].x);
-                    float ssum = 0.f;
-                    for (int k = 0; k < C; ++k) {
-                        const float2 ps = xch[(slot * kMaxCluster + k) * R + r];
-                        if (ps.x != -INFINITY) ssum += ps.y * ex2((ps.x - m) * kLog2e);
-                    }
-                    M[r] = m;
-                    S[r] = ssum;
-                }
+            slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status);
+            if (!agree(slot >= 0)) {
+                alive = false;
+                break;
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const float lse = M[r] + logf(S[r]);
+                const float S = slot_sum<THREADS, R>(xch, slot, C, r);
+                const float lse = M[r] + logf(S);
                 anew[r] = momentum ? (1.f - omega) * a_old[r] - omega * lse : -lse;
-                wr[r] = (Mc[r] == -INFINITY) ? 0.f : ex2((Mc[r] + anew[r]) * kLog2e);
+                wr[r] = (M[r] == -INFINITY) ? 0.f : ex2((M[r] + anew[r]) * kLog2e);
             }
         }
-        // Stage s is no longer read by the row reduction; the absorb variant
-        // still re-reads it below.
-        if (!ABSORB) release(bt);
         if (rank == 0 && tid < rows) {
             float v = anew[0];
 #pragma unroll
@@ -525,7 +518,6 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
         }
         if (ABSORB) {
             // cost16 = cost32 + b_j + a_i  (~ log P after this row update), rounded once
-            constexpr int VO = V;  // T is float here: 4 outputs per chunk
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int c = (g * THREADS + tid) * V;
@@ -537,9 +529,9 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
                                 *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
                             float vals[V];
                             Vec<T>::unpack(raw, vals);
-                            TOUT o[VO];
+                            TOUT o[V];
 #pragma unroll
-                            for (int q = 0; q < VO; ++q)
+                            for (int q = 0; q < V; ++q)
                                 o[q] = from_float<TOUT>((c + q < nvalid) ? vals[q] + b_s[c + q] + anew[r]
                                                                          : -INFINITY);
                             TOUT* dst = static_cast<TOUT*>(p.out16) + static_cast<size_t>(r0 + r) * p.ld16 + col0 + c;
@@ -576,7 +568,9 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(const SweepArgs p) {
         for (int b = bt; b < issued; ++b)
             if (!mbar_wait(&full[b % p.stages], static_cast<uint32_t>((b / p.stages) & 1), &st->status)) break;
     }
-    if (C > 1) cluster_sync();  // no CTA leaves while a peer may still write its shared memory
+    // No CTA leaves while a peer may still send into its shared memory; the
+    // non-aligned form tolerates threads that left the batch loop early.
+    cluster_sync_any();
 }
 
 // Reduce the per-cluster column sums (FP64), write log(colsum), decide.
@@ -824,9 +818,9 @@ int elem_size(int dt) { return dt == FUGAL_F32 ? 4 : 2; }
 
 using KernelFn = void (*)(const SweepArgs);
 
-// Rows per batch: 4 for 16-bit streams up to 256 threads, else 2 (keeps the
-// 16 x R exponentials of a thread in registers without spilling at 512 threads).
-constexpr int rows_per_batch(int elem_bytes, int threads) { return (elem_bytes == 4 || threads == 512) ? 2 : 4; }
+// Rows per batch: 2 (the 16 x R exponentials of a thread stay in registers
+// within a 128-register budget).
+constexpr int rows_per_batch(int elem_bytes, int threads) { return (void)elem_bytes, (void)threads, 2; }
 
 template <typename T, int THREADS, bool ABSORB, typename TOUT>
 KernelFn pick_kernel() {
@@ -851,9 +845,9 @@ KernelFn kernel_for(int threads, int dt, int kind) {
 }
 
 int header_for(int threads, int R) {
-    if (threads == 128) return R == 2 ? header_bytes<128, 2>() : header_bytes<128, 4>();
-    if (threads == 256) return R == 2 ? header_bytes<256, 2>() : header_bytes<256, 4>();
-    return R == 2 ? header_bytes<512, 2>() : header_bytes<512, 4>();
+    if (threads == 128) return R == 2 ? header_bytes_v3<128, 2>() : header_bytes_v3<128, 4>();
+    if (threads == 256) return R == 2 ? header_bytes_v3<256, 2>() : header_bytes_v3<256, 4>();
+    return R == 2 ? header_bytes_v3<512, 2>() : header_bytes_v3<512, 4>();
 }
 
 int max_smem_optin() {
@@ -864,21 +858,19 @@ int max_smem_optin() {
     return v;
 }
 
-// Largest column slice per CTA (THREADS * 16): 8192 by default; the
-// environment variable FUGAL_SWEEP_SLICE (2048, 4096 or 8192) lowers it, which
-// trades larger clusters for fewer threads per CTA.
+// Column slice per CTA (THREADS * 16): 4096 by default (256 threads, two CTAs
+// per SM); the environment variable FUGAL_SWEEP_SLICE (2048, 4096 or 8192)
+// overrides it, trading cluster size against threads per CTA.
 int max_slice() {
     const char* e = getenv("FUGAL_SWEEP_SLICE");
-    const int v = e ? atoi(e) : 8192;
-    return (v == 2048 || v == 4096) ? v : 8192;
+    const int v = e ? atoi(e) : 4096;
+    return (v == 2048 || v == 8192) ? v : 4096;
 }
 
 // Launch shape for n columns: threads per CTA and CTAs per cluster, so that
-// cluster * threads * 16 >= n with the smallest cluster.
+// cluster * threads * 16 >= n with the smallest power-of-two cluster.
 fugal_status plan_shape(int64_t n, int& threads, int& cluster) {
-    if (n <= 2048) { threads = 128; cluster = 1; return FUGAL_OK; }
-    if (n <= 4096 && max_slice() >= 4096) { threads = 256; cluster = 1; return FUGAL_OK; }
-    const int slice = max_slice();
+    const int slice = n <= 2048 ? 2048 : max_slice();
     threads = slice / kKPT;
     cluster = 1;
     while (static_cast<int64_t>(cluster) * slice < n) cluster <<= 1;
@@ -888,6 +880,10 @@ fugal_status plan_shape(int64_t n, int& threads, int& cluster) {
     return FUGAL_OK;
 }
 
+// Dynamic shared memory per CTA kept near 100 KB so two CTAs (of up to 256
+// threads) share an SM and hide each other's exchange latency.
+constexpr int kSmemTarget = 100 * 1024;
+
 fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_occupancy) {
     FUGAL_TRY(plan_shape(n, pl.threads, pl.cluster));
     const int es = (kind != 0) ? 4 : elem_size(dt);
@@ -895,10 +891,10 @@ fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_oc
     pl.slice_w = pl.threads * kKPT;
     const size_t stage_bytes = static_cast<size_t>(pl.R) * pl.slice_w * es;
     const size_t fixed = header_for(pl.threads, pl.R) + static_cast<size_t>(pl.slice_w) * 4;
-    const int budget = max_smem_optin();
+    const int budget = pl.threads >= 512 ? max_smem_optin() : kSmemTarget;
     int stages = static_cast<int>((budget - static_cast<int64_t>(fixed)) / static_cast<int64_t>(stage_bytes));
     stages = std::min(stages, kMaxStages);
-    if (pl.threads < 512) stages = std::min(stages, 4);  // small slices: leave room for 2+ CTAs per SM
+    if (stages < 2) stages = std::min(2, static_cast<int>((max_smem_optin() - fixed) / stage_bytes));
     if (stages < 1) return fail(FUGAL_BAD_SHAPE, "sinkhorn: no shared-memory stage fits");
     pl.stages = stages;
     pl.smem = fixed + stages * stage_bytes;
@@ -1022,6 +1018,21 @@ extern "C" fugal_status fugal_sinkhorn_workspace_size(int64_t n, int stream_dtyp
     int threads, cluster;
     FUGAL_TRY(plan_shape(n, threads, cluster));
     *bytes = layout(n, nullptr, partial_rows_bound(n)).bytes;
+    return FUGAL_OK;
+}
+
+extern "C" fugal_status fugal_sinkhorn_plan_info(int64_t n, int stream_dtype, int32_t* info) {
+    if (info == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_plan_info: null output");
+    if (stream_dtype < FUGAL_F32 || stream_dtype > FUGAL_F16)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_plan_info: bad stream dtype");
+    SweepPlan pl;
+    FUGAL_TRY(make_plan(n, stream_dtype, 0, pl, true));
+    info[0] = pl.threads;
+    info[1] = pl.cluster;
+    info[2] = pl.clusters;
+    info[3] = pl.stages;
+    info[4] = static_cast<int32_t>(pl.smem);
+    info[5] = pl.R;
     return FUGAL_OK;
 }
 

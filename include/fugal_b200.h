@@ -212,6 +212,10 @@ typedef struct {
 } fugal_solve_record;
 
 fugal_status fugal_sinkhorn_workspace_size(int64_t n, int stream_dtype, size_t* bytes);
+/* Launch shape of the sweeps over an n-column cost of stream_dtype on the
+ * current device: info = {threads per CTA, CTAs per cluster, clusters in the
+ * grid, pipeline stages, dynamic shared memory bytes, rows per batch}. */
+fugal_status fugal_sinkhorn_plan_info(int64_t n, int stream_dtype, int32_t* info);
 fugal_status fugal_sinkhorn_solve(const fugal_solve_params* params, void* workspace, size_t workspace_bytes,
                                   fugal_stream_t stream);
 

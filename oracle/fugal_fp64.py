@@ -413,9 +413,10 @@ def greedy_lap(P: np.ndarray, method: str, order=None, uniforms=None):
     raise ValueError(method)
 
 
-def sparsity(P: np.ndarray) -> float:
-    """Fraction of entries <= machine epsilon (``cugal/pred.py:152-153``)."""
-    return float(np.sum(P <= np.finfo(P.dtype).eps)) / P.size
+def sparsity(P: np.ndarray, eps: float | None = None) -> float:
+    """Fraction of entries <= machine epsilon of P's dtype (``cugal/pred.py:152-153``)."""
+    eps = np.finfo(P.dtype).eps if eps is None else eps
+    return float(np.sum(P <= eps)) / P.size
 
 
 def hungarian(P: np.ndarray, method: str, **kw) -> np.ndarray:
@@ -503,7 +504,8 @@ def pad_graphs(source, target):
     target.add_nodes_from(set(range(node_count)) - set(target.nodes()))
 
 
-def cugal(source, target, p: OracleParams, features: str = "cuda", trace: FWTrace | None = None, **lap_kw):
+def cugal(source, target, p: OracleParams, features: str = "cuda", trace: FWTrace | None = None,
+          sparsity_eps: float | None = None, **lap_kw):
     """``cugal`` (``cugal/pred.py:196-249``): returns (P, mapping, sparsity).
 
     ``features='cuda'`` uses the integer-count semantics of the CUDA kernels
@@ -518,7 +520,7 @@ def cugal(source, target, p: OracleParams, features: str = "cuda", trace: FWTrac
         F1, F2 = features_nx_semantics(source), features_nx_semantics(target)
     D = distance_matrix(p.mu * F1, p.mu * F2)
     P = find_quasi_permutation_matrix(A_csr, B_csr, D, p, trace)
-    sp = sparsity(P)
+    sp = sparsity(P, sparsity_eps)
     cols = hungarian(P, p.hungarian_method, **lap_kw)
     mapping = [(i, int(cols[i])) for i in range(len(P))]
     return P, mapping, sp

@@ -139,7 +139,7 @@ def test_sinkhorn_momentum_matches_oracle():
     ref = O.sinkhorn_log_solve(C, zero, zero, 0.05, 300, 1e-4, 5, momentum_start=10)
     u, v, prof = _solve_gpu(C, zero, zero, 0.05, 300, 1e-4, 5, mstart=10)
     assert prof.iteration_count == ref.iteration_count
-    np.testing.assert_allclose(prof.errors, ref.errors, rtol=2e-2)
+    np.testing.assert_allclose(prof.errors, ref.errors, rtol=2e-2, atol=5e-8 * n)
     np.testing.assert_allclose(_plan(C, u, v, 0.05), _plan(C, ref.u, ref.v, 0.05), atol=2e-4)
 
 
@@ -239,17 +239,17 @@ def test_full_alignment_matches_oracle(lap):
     prof = Profile()
     P, mapping = cugal(nx.Graph(g), nx.Graph(h), cfg, prof)
     trace = O.FWTrace()
-    Pr, mref, sp = O.cugal(nx.Graph(g), nx.Graph(h),
-                           O.OracleParams(sinkhorn_method="LOG", use_sparse_adjacency=True, hungarian_method=lap,
-                                          **params), features="cuda", trace=trace)
+    Pr, mref, sp32 = O.cugal(nx.Graph(g), nx.Graph(h),
+                             O.OracleParams(sinkhorn_method="LOG", use_sparse_adjacency=True, hungarian_method=lap,
+                                            **params), features="cuda", trace=trace,
+                             sparsity_eps=float(np.finfo(np.float32).eps))
     assert prof.frank_wolfe_iterations == trace.frank_wolfe_iterations == 30
     its = [p.iteration_count for p in prof.sinkhorn_profiles]
     assert len(its) == 30
     assert max(abs(a - b) for a, b in zip(its, trace.sinkhorn_iterations)) <= 10
     assert [m[1] for m in mapping] == [m[1] for m in mref]
     np.testing.assert_allclose(P, Pr, atol=2e-3)
-    # the reference's GPU path counts entries <= FP32 epsilon (its P is FP32)
-    sp32 = float(np.sum(Pr <= np.finfo(np.float32).eps)) / Pr.size
+    # the reference's GPU path counts entries <= FP32 epsilon (its P is FP32), before rounding
     assert abs(prof.sparsity - sp32) < 0.02
     from cugal_b200 import Phase
     assert set(prof.phase_times) == set(Phase)

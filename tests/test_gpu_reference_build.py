@@ -3,7 +3,7 @@ the reference sources by oracle/build_ref.py) on identical inputs.
 
 The reference compiles with --use_fast_math, so its float divisions, square
 roots and exponentials are approximate: integer results are compared exactly,
-ratios within 2 ulp, LSE / update results within 1e-5 relative.
+ratios within 4 ulp, LSE / update results within 1e-5 relative.
 """
 
 import networkx as nx
@@ -49,7 +49,7 @@ def test_features_against_reference_kernels(name, graph):
         outs[tag] = [t.cpu().numpy() for t in (deg, clust, nd, nc)]
     assert np.array_equal(outs["ref"][0], outs["ours"][0])          # degrees exact
     for k in (1, 2, 3):
-        assert _ulps(outs["ref"][k], outs["ours"][k]).max() <= 2     # fast-math divisions
+        assert _ulps(outs["ref"][k], outs["ours"][k]).max() <= 4     # fast-math divisions
 
 
 def test_csr_against_reference_kernel():
