@@ -139,6 +139,7 @@ struct SweepArgs {
     int n_copy;           // columns copied per row (multiple of 16 bytes)
     int slice_w;          // columns per CTA = THREADS * kKPT
     int rows_per_cluster;
+    int rows_pad;         // rows_per_cluster rounded up to 32 (shared staging of the row duals)
     int stages;
     const float* b_buf;   // [2][n_pad] column duals of consecutive sweeps
     const float* b_off;   // frame offset added to the previous b (nullable)
@@ -250,7 +251,8 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     uint64_t* xbar = full + kMaxStages;
     float2* xch = reinterpret_cast<float2*>(smem + kBarBytes);
     float* b_s = reinterpret_cast<float*>(smem + header_bytes_v3<THREADS, R>());
-    unsigned char* stage_base = reinterpret_cast<unsigned char*>(b_s + p.slice_w);
+    float* a_s = b_s + p.slice_w;  // previous row duals of this cluster's rows
+    unsigned char* stage_base = reinterpret_cast<unsigned char*>(a_s + p.rows_pad);
 
     SolveState* st = p.st;
     if (*reinterpret_cast<volatile int*>(&st->done)) return;  // uniform: written by an earlier kernel
@@ -292,6 +294,13 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
             }
         }
         b_s[j] = b;
+    }
+    // Row duals of the previous sweep (the fast path's exponent reference and
+    // the momentum term), read once here instead of on every batch's critical path.
+    for (int i = tid; i < row_end - row_begin; i += THREADS) {
+        float a = p.a[row_begin + i];
+        if (p.a_off != nullptr) a += p.a_off[row_begin + i];
+        a_s[i] = a;
     }
     if (tid == 0) {
         for (int s = 0; s < p.stages; ++s) mbar_init(&full[s], 1);
@@ -358,13 +367,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
         float e[R][kKPT];
         float anew[R], wr[R], a_old[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            a_old[r] = 0.f;
-            if (r < rows) {
-                a_old[r] = p.a[r0 + r];
-                if (p.a_off != nullptr) a_old[r] += p.a_off[r0 + r];
-            }
-        }
+        for (int r = 0; r < R; ++r) a_old[r] = (r < rows) ? a_s[bt * R + r] : 0.f;
         bool fast_ok = false;
         if (!exact_only) {
             // ---- fast path: exponents relative to the previous row normaliser -a_old
@@ -810,6 +813,7 @@ struct SweepPlan {
     int slice_w;
     int clusters;       // number of clusters in the grid
     int rows_per_cluster;
+    int rows_pad;
     int stages;
     size_t smem;
 };
@@ -890,46 +894,55 @@ fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_oc
     pl.R = rows_per_batch(es, pl.threads);
     pl.slice_w = pl.threads * kKPT;
     const size_t stage_bytes = static_cast<size_t>(pl.R) * pl.slice_w * es;
-    const size_t fixed = header_for(pl.threads, pl.R) + static_cast<size_t>(pl.slice_w) * 4;
-    const int budget = pl.threads >= 512 ? max_smem_optin() : kSmemTarget;
-    int stages = static_cast<int>((budget - static_cast<int64_t>(fixed)) / static_cast<int64_t>(stage_bytes));
-    stages = std::min(stages, kMaxStages);
-    if (stages < 2) stages = std::min(2, static_cast<int>((max_smem_optin() - fixed) / stage_bytes));
-    if (stages < 1) return fail(FUGAL_BAD_SHAPE, "sinkhorn: no shared-memory stage fits");
-    pl.stages = stages;
-    pl.smem = fixed + stages * stage_bytes;
     const int sms = sm_count();
-    int clusters = sms / pl.cluster;
-    if (query_occupancy) {
-        KernelFn fn = kernel_for(pl.threads, dt, kind);
-        FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem),
-                             "sinkhorn: set dynamic shared memory"));
-        if (pl.cluster > 8)
-            FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
-                                 "sinkhorn: allow cluster size 16"));
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute attr[1];
-        cfg.gridDim = dim3(pl.cluster, 1, 1);
-        cfg.blockDim = dim3(pl.threads, 1, 1);
-        cfg.dynamicSmemBytes = pl.smem;
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = pl.cluster;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        int active = 0;
-        FUGAL_TRY(cuda_check(cudaOccupancyMaxActiveClusters(&active, fn, &cfg), "sinkhorn: occupancy query"));
-        if (active <= 0) return fail(FUGAL_UNSUPPORTED, "sinkhorn: cluster of %d CTAs cannot be scheduled", pl.cluster);
-        clusters = active;
-    } else {
-        clusters = sms * 4;  // upper bound for workspace sizing
+    const int ctas_per_sm = pl.threads >= 512 ? 1 : 2;
+    // clusters the grid is expected to hold; the row-dual staging is sized from it
+    int est = std::max(1, (sms * ctas_per_sm / pl.cluster) * 3 / 4);
+    KernelFn fn = kernel_for(pl.threads, dt, kind);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        pl.rows_pad = static_cast<int>(((n + est - 1) / est + 31) / 32 * 32);
+        const size_t fixed = header_for(pl.threads, pl.R) + static_cast<size_t>(pl.slice_w) * 4 +
+                             static_cast<size_t>(pl.rows_pad) * 4;
+        const int budget = pl.threads >= 512 ? max_smem_optin() : kSmemTarget;
+        int stages = static_cast<int>((budget - static_cast<int64_t>(fixed)) / static_cast<int64_t>(stage_bytes));
+        stages = std::min(stages, kMaxStages);
+        if (stages < 2) stages = std::min(2, static_cast<int>((max_smem_optin() - static_cast<int64_t>(fixed)) /
+                                                               static_cast<int64_t>(stage_bytes)));
+        if (stages < 1) return fail(FUGAL_BAD_SHAPE, "sinkhorn: no shared-memory stage fits");
+        pl.stages = stages;
+        pl.smem = fixed + stages * stage_bytes;
+        int clusters = sms * 4;  // upper bound for workspace sizing
+        if (query_occupancy) {
+            FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem),
+                                 "sinkhorn: set dynamic shared memory"));
+            if (pl.cluster > 8)
+                FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+                                     "sinkhorn: allow cluster size 16"));
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            cfg.gridDim = dim3(pl.cluster, 1, 1);
+            cfg.blockDim = dim3(pl.threads, 1, 1);
+            cfg.dynamicSmemBytes = pl.smem;
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = pl.cluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int active = 0;
+            FUGAL_TRY(cuda_check(cudaOccupancyMaxActiveClusters(&active, fn, &cfg), "sinkhorn: occupancy query"));
+            if (active <= 0)
+                return fail(FUGAL_UNSUPPORTED, "sinkhorn: cluster of %d CTAs cannot be scheduled", pl.cluster);
+            clusters = active;
+        }
+        const int max_useful = static_cast<int>((n + pl.R - 1) / pl.R);
+        clusters = std::max(1, std::min(clusters, max_useful));
+        pl.clusters = clusters;
+        pl.rows_per_cluster = static_cast<int>((n + clusters - 1) / clusters);
+        if (pl.rows_per_cluster <= pl.rows_pad) return FUGAL_OK;
+        est = clusters;  // fewer clusters than estimated: size the staging for them and re-plan
     }
-    const int max_useful = static_cast<int>((n + pl.R - 1) / pl.R);
-    clusters = std::max(1, std::min(clusters, max_useful));
-    pl.clusters = clusters;
-    pl.rows_per_cluster = static_cast<int>((n + clusters - 1) / clusters);
-    return FUGAL_OK;
+    return fail(FUGAL_UNSUPPORTED, "sinkhorn: could not fit the row-dual staging for n = %lld", (long long)n);
 }
 
 constexpr int kColThreads = 256;
@@ -1109,6 +1122,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         a.n_copy = static_cast<int>((n + V - 1) / V * V);
         a.slice_w = pl.slice_w;
         a.rows_per_cluster = pl.rows_per_cluster;
+        a.rows_pad = pl.rows_pad;
         a.stages = pl.stages;
         a.b_buf = w.b_buf;
         a.b_buf_w = w.b_buf;
