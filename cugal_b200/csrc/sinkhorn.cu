@@ -51,7 +51,6 @@ namespace fugal {
 
 constexpr int kMaxStages = 8;
 constexpr int kMaxCluster = 16;
-constexpr int kKPT = 16;  // columns per thread
 
 struct SolveState {
     int it;          // index of the next sweep
@@ -137,7 +136,7 @@ struct SweepArgs {
     long long ld;
     int n;
     int n_copy;           // columns copied per row (multiple of 16 bytes)
-    int slice_w;          // columns per CTA = THREADS * kKPT
+    int slice_w;          // columns per CTA = threads x columns per thread
     int rows_per_cluster;
     int rows_pad;         // rows_per_cluster rounded up to 32 (shared staging of the row duals)
     int stages;
@@ -240,11 +239,42 @@ __device__ __forceinline__ float slot_sum(const float2* xch, int slot, int C, in
     return lanes_sum(v);
 }
 
-// At most 128 registers per thread so that 512 threads' worth of CTAs share an SM.
-template <typename T, int THREADS, int R, bool ABSORB, typename TOUT>
+// One 16-byte chunk of T as float pairs (elements 2q, 2q+1 in .x, .y).
+template <typename T> struct Pairs;
+template <> struct Pairs<float> {
+    FUGAL_DEVICE static void unpack(const uint4& r, float2* o) {
+        o[0] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+        o[1] = make_float2(__uint_as_float(r.z), __uint_as_float(r.w));
+    }
+};
+template <> struct Pairs<__nv_bfloat16> {
+    FUGAL_DEVICE static void unpack(const uint4& r, float2* o) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o[i] = make_float2(__uint_as_float(w[i] << 16), __uint_as_float(w[i] & 0xffff0000u));
+    }
+};
+template <> struct Pairs<__half> {
+    FUGAL_DEVICE static void unpack(const uint4& r, float2* o) {
+        const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o[i] = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
+    }
+};
+
+FUGAL_DEVICE float2 ex2_pair(float2 x) { return make_float2(ex2(x.x), ex2(x.y)); }
+
+// Sweep kernel.  Each thread owns KPT columns of its CTA's slice as KPT/2
+// float pairs and processes R rows per batch; the hot loop runs on Blackwell's
+// packed FP32x2 FMA/ADD (fma.rn.f32x2) with the exponentials on MUFU ex2, in
+// base-2 units (b_s holds the column duals times log2 e).  At most 128
+// registers per thread so two 256-thread CTAs share an SM.
+template <typename T, int THREADS, int KPT, int R, bool ABSORB, typename TOUT>
 __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS)) sweep_kernel(const SweepArgs p) {
-    constexpr int V = Vec<T>::N;
-    constexpr int G = kKPT / V;
+    constexpr int V = Vec<T>::N;  // elements per 16-byte chunk
+    constexpr int G = KPT / V;    // chunks per thread per row
+    constexpr int VP = V / 2;     // pairs per chunk
+    constexpr int H = KPT / 2;    // pairs per thread per row
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int abort_s;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
@@ -265,6 +295,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     const int col0 = rank * p.slice_w;
     const int ncopy = max(0, min(p.slice_w, p.n_copy - col0));
     const int nvalid = max(0, min(p.slice_w, n - col0));
+    const bool full_slice = nvalid == p.slice_w;  // uniform per CTA: no column masking needed
     const int row_begin = cid * p.rows_per_cluster;
     const int row_end = min(n, row_begin + p.rows_per_cluster);
     const int nbatch = row_end > row_begin ? (row_end - row_begin + R - 1) / R : 0;
@@ -276,8 +307,9 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     const size_t stage_bytes = static_cast<size_t>(R) * p.slice_w * sizeof(T);
     const float* b_prev = p.b_buf + ((t - 1) & 1) * p.n_pad;
     float* b_out = p.b_buf_w + (t & 1) * p.n_pad;
+    const float2 log2e2 = make_float2(kLog2e, kLog2e);
 
-    // Column duals of this sweep: b = b_off + b_prev - w log(colsum_prev).
+    // Column duals of this sweep: b = b_off + b_prev - w log(colsum_prev); kept as b * log2 e.
     for (int j = tid; j < p.slice_w; j += THREADS) {
         float b = 0.f;
         if (j < nvalid) {
@@ -293,7 +325,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                 }
             }
         }
-        b_s[j] = b;
+        b_s[j] = b * kLog2e;
     }
     // Row duals of the previous sweep (the fast path's exponent reference and
     // the momentum term), read once here instead of on every batch's critical path.
@@ -346,10 +378,19 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
         if (!ok) abort_s = 1;
         return ok && *reinterpret_cast<volatile int*>(&abort_s) == 0;
     };
-
-    float acc[kKPT];
+    // b * log2e for the pairs of chunk g of this thread.
+    auto load_b2 = [&](int c, float2* b2) {
 #pragma unroll
-    for (int k = 0; k < kKPT; ++k) acc[k] = 0.f;
+        for (int q = 0; q < VP; q += 2) {
+            const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + 2 * q);
+            b2[q] = make_float2(b4.x, b4.y);
+            b2[q + 1] = make_float2(b4.z, b4.w);
+        }
+    };
+
+    float2 acc[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) acc[h] = make_float2(0.f, 0.f);
 
     int xuse = 0;
     bool alive = true;
@@ -364,49 +405,48 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
         const int rows = min(R, row_end - r0);
         const T* stage = reinterpret_cast<const T*>(stage_base + s * stage_bytes);
 
-        float e[R][kKPT];
+        float2 e[R][H];
         float anew[R], wr[R], a_old[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) a_old[r] = (r < rows) ? a_s[bt * R + r] : 0.f;
         bool fast_ok = false;
         if (!exact_only) {
-            // ---- fast path: exponents relative to the previous row normaliser -a_old
-            float mref2[R], sm[R], zero[R];
+            // ---- fast path: exponents relative to the previous row normaliser -a_old:
+            //      e = 2^(L log2e + b2 + a_old log2e)
+            float sm[R], zero[R];
+            float2 s2[R], ref2[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                mref2[r] = -a_old[r] * kLog2e;
-                sm[r] = 0.f;
+                ref2[r] = make_float2(a_old[r] * kLog2e, a_old[r] * kLog2e);
+                s2[r] = make_float2(0.f, 0.f);
                 zero[r] = 0.f;
             }
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int c = (g * THREADS + tid) * V;
-                float bv[V];
-#pragma unroll
-                for (int q = 0; q < V; q += 4) {
-                    const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + q);
-                    bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
-                }
-                const bool whole = c + V <= nvalid;
+                float2 b2[VP];
+                load_b2(c, b2);
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (r < rows) {
-                        const uint4 raw =
-                            *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
-                        float vals[V];
-                        Vec<T>::unpack(raw, vals);
+                        float2 v2[VP];
+                        Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c),
+                                         v2);
 #pragma unroll
-                        for (int q = 0; q < V; ++q) {
-                            float y = ex2(fmaf(vals[q] + bv[q], kLog2e, -mref2[r]));
-                            if (!whole && c + q >= nvalid) y = 0.f;
-                            e[r][g * V + q] = y;
-                            sm[r] += y;
+                        for (int q = 0; q < VP; ++q) {
+                            float2 y = ex2_pair(__ffma2_rn(v2[q], log2e2, __fadd2_rn(b2[q], ref2[r])));
+                            if (!full_slice) {
+                                if (c + 2 * q >= nvalid) y.x = 0.f;
+                                if (c + 2 * q + 1 >= nvalid) y.y = 0.f;
+                            }
+                            e[r][g * VP + q] = y;
+                            s2[r] = __fadd2_rn(s2[r], y);
                         }
                     }
                 }
             }
 #pragma unroll
-            for (int r = 0; r < R; ++r) sm[r] = warp_sum(sm[r]);
+            for (int r = 0; r < R; ++r) sm[r] = warp_sum(s2[r].x + s2[r].y);
             const int slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status);
             if (!agree(slot >= 0)) {
                 alive = false;
@@ -422,14 +462,14 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
             if (fast_ok) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    anew[r] = a_old[r] - logf(S[r]);  // -(M_ref + log S)
-                    wr[r] = 1.0f / S[r];
+                    anew[r] = a_old[r] - __log2f(S[r]) * kLn2;  // -(M_ref + ln S)
+                    wr[r] = __frcp_rn(S[r]);
                 }
                 if (!ABSORB) release(bt);
             }
         }
         if (!fast_ok) {
-            // ---- exact path: cluster-wide row maximum first, then the exponentials
+            // ---- exact path (base 2): cluster-wide row maximum first, then the exponentials
             float mx[R], zero[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -439,28 +479,25 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int c = (g * THREADS + tid) * V;
-                float bv[V];
-#pragma unroll
-                for (int q = 0; q < V; q += 4) {
-                    const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + q);
-                    bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
-                }
+                float2 b2[VP];
+                load_b2(c, b2);
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (r < rows) {
-                        const uint4 raw =
-                            *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
-                        float vals[V];
-                        Vec<T>::unpack(raw, vals);
+                        float2 v2[VP];
+                        Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c),
+                                         v2);
 #pragma unroll
-                        for (int q = 0; q < V; ++q) {
-                            const float x = (c + q < nvalid) ? vals[q] + bv[q] : -INFINITY;
-                            e[r][g * V + q] = x;
-                            mx[r] = fmaxf(mx[r], x);
+                        for (int q = 0; q < VP; ++q) {
+                            float2 x = __ffma2_rn(v2[q], log2e2, b2[q]);
+                            if (c + 2 * q >= nvalid) x.x = -INFINITY;
+                            if (c + 2 * q + 1 >= nvalid) x.y = -INFINITY;
+                            e[r][g * VP + q] = x;
+                            mx[r] = fmaxf(mx[r], fmaxf(x.x, x.y));
                         }
                     } else {
 #pragma unroll
-                        for (int q = 0; q < V; ++q) e[r][g * V + q] = -INFINITY;
+                        for (int q = 0; q < VP; ++q) e[r][g * VP + q] = make_float2(-INFINITY, -INFINITY);
                     }
                 }
             }
@@ -472,19 +509,20 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                 break;
             }
             if (!ABSORB) release(bt);
-            float M[R], M2[R], sm[R];
+            float M2[R], sm[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                M[r] = slot_max<THREADS, R>(xch, slot, C, r);
-                M2[r] = (M[r] == -INFINITY) ? 0.f : M[r] * kLog2e;
-                float ssum = 0.f;
+                M2[r] = slot_max<THREADS, R>(xch, slot, C, r);
+                const float base = (M2[r] == -INFINITY) ? 0.f : M2[r];
+                const float2 nb = make_float2(-base, -base);
+                float2 ss = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int k = 0; k < kKPT; ++k) {
-                    const float y = ex2(fmaf(e[r][k], kLog2e, -M2[r]));
-                    e[r][k] = y;
-                    ssum += y;
+                for (int h = 0; h < H; ++h) {
+                    const float2 y = ex2_pair(__fadd2_rn(e[r][h], nb));
+                    e[r][h] = y;
+                    ss = __fadd2_rn(ss, y);
                 }
-                sm[r] = warp_sum(ssum);
+                sm[r] = warp_sum(ss.x + ss.y);
             }
             slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status);
             if (!agree(slot >= 0)) {
@@ -494,9 +532,10 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const float S = slot_sum<THREADS, R>(xch, slot, C, r);
-                const float lse = M[r] + logf(S);
+                const float lse = (M2[r] + log2f(S)) * kLn2;
                 anew[r] = momentum ? (1.f - omega) * a_old[r] - omega * lse : -lse;
-                wr[r] = (M[r] == -INFINITY) ? 0.f : ex2((M[r] + anew[r]) * kLog2e);
+                // P = e * 2^(M2) * e^(anew)
+                wr[r] = (M2[r] == -INFINITY) ? 0.f : ex2(M2[r] + anew[r] * kLog2e);
             }
         }
         if (rank == 0 && tid < rows) {
@@ -515,8 +554,9 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (r < rows) {
+                const float2 w2 = make_float2(wr[r], wr[r]);
 #pragma unroll
-                for (int k = 0; k < kKPT; ++k) acc[k] = fmaf(e[r][k], wr[r], acc[k]);
+                for (int h = 0; h < H; ++h) acc[h] = __ffma2_rn(e[r][h], w2, acc[h]);
             }
         }
         if (ABSORB) {
@@ -535,7 +575,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                             TOUT o[V];
 #pragma unroll
                             for (int q = 0; q < V; ++q)
-                                o[q] = from_float<TOUT>((c + q < nvalid) ? vals[q] + b_s[c + q] + anew[r]
+                                o[q] = from_float<TOUT>((c + q < nvalid) ? vals[q] + b_s[c + q] * kLn2 + anew[r]
                                                                          : -INFINITY);
                             TOUT* dst = static_cast<TOUT*>(p.out16) + static_cast<size_t>(r0 + r) * p.ld16 + col0 + c;
                             *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(o);
@@ -555,13 +595,15 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
         const int c = (g * THREADS + tid) * V;
         if (c + V <= nvalid) {
 #pragma unroll
-            for (int q = 0; q < V; q += 4)
-                *reinterpret_cast<float4*>(prow + c + q) =
-                    make_float4(acc[g * V + q], acc[g * V + q + 1], acc[g * V + q + 2], acc[g * V + q + 3]);
+            for (int q = 0; q < VP; q += 2)
+                *reinterpret_cast<float4*>(prow + c + 2 * q) =
+                    make_float4(acc[g * VP + q].x, acc[g * VP + q].y, acc[g * VP + q + 1].x, acc[g * VP + q + 1].y);
         } else {
 #pragma unroll
-            for (int q = 0; q < V; ++q)
-                if (c + q < nvalid) prow[c + q] = acc[g * V + q];
+            for (int q = 0; q < VP; ++q) {
+                if (c + 2 * q < nvalid) prow[c + 2 * q] = acc[g * VP + q].x;
+                if (c + 2 * q + 1 < nvalid) prow[c + 2 * q + 1] = acc[g * VP + q].y;
+            }
         }
     }
 
@@ -808,6 +850,7 @@ namespace {
 
 struct SweepPlan {
     int threads;
+    int kpt;
     int R;
     int cluster;
     int slice_w;
@@ -822,36 +865,35 @@ int elem_size(int dt) { return dt == FUGAL_F32 ? 4 : 2; }
 
 using KernelFn = void (*)(const SweepArgs);
 
-// Rows per batch: 2 (the 16 x R exponentials of a thread stay in registers
-// within a 128-register budget).
-constexpr int rows_per_batch(int elem_bytes, int threads) { return (void)elem_bytes, (void)threads, 2; }
+// Launch shapes: (threads per CTA, columns per thread).  Rows per batch are
+// 32 / columns-per-thread, so a thread always holds 32 exponentials.
+constexpr int rows_per_batch(int kpt) { return 32 / kpt; }
 
-template <typename T, int THREADS, bool ABSORB, typename TOUT>
+using KernelFn = void (*)(const SweepArgs);
+
+template <typename T, int THREADS, int KPT, bool ABSORB, typename TOUT>
 KernelFn pick_kernel() {
-    constexpr int R = rows_per_batch(sizeof(T), THREADS);
-    return sweep_kernel<T, THREADS, R, ABSORB, TOUT>;
+    return sweep_kernel<T, THREADS, KPT, rows_per_batch(KPT), ABSORB, TOUT>;
 }
 
 // kind: 0 = plain sweep over dtype dt, 1 = absorb (fp32 -> bf16), 2 = absorb (fp32 -> fp16)
-template <int THREADS>
+template <int THREADS, int KPT>
 KernelFn kernel_for(int dt, int kind) {
-    if (kind == 1) return pick_kernel<float, THREADS, true, __nv_bfloat16>();
-    if (kind == 2) return pick_kernel<float, THREADS, true, __half>();
-    if (dt == FUGAL_BF16) return pick_kernel<__nv_bfloat16, THREADS, false, float>();
-    if (dt == FUGAL_F16) return pick_kernel<__half, THREADS, false, float>();
-    return pick_kernel<float, THREADS, false, float>();
+    if (kind == 1) return pick_kernel<float, THREADS, KPT, true, __nv_bfloat16>();
+    if (kind == 2) return pick_kernel<float, THREADS, KPT, true, __half>();
+    if (dt == FUGAL_BF16) return pick_kernel<__nv_bfloat16, THREADS, KPT, false, float>();
+    if (dt == FUGAL_F16) return pick_kernel<__half, THREADS, KPT, false, float>();
+    return pick_kernel<float, THREADS, KPT, false, float>();
 }
 
-KernelFn kernel_for(int threads, int dt, int kind) {
-    if (threads == 128) return kernel_for<128>(dt, kind);
-    if (threads == 256) return kernel_for<256>(dt, kind);
-    return kernel_for<512>(dt, kind);
+KernelFn kernel_for(int threads, int kpt, int dt, int kind) {
+    if (threads == 128) return kpt == 16 ? kernel_for<128, 16>(dt, kind) : kernel_for<128, 32>(dt, kind);
+    return kpt == 16 ? kernel_for<256, 16>(dt, kind) : kernel_for<256, 32>(dt, kind);
 }
 
 int header_for(int threads, int R) {
-    if (threads == 128) return R == 2 ? header_bytes_v3<128, 2>() : header_bytes_v3<128, 4>();
-    if (threads == 256) return R == 2 ? header_bytes_v3<256, 2>() : header_bytes_v3<256, 4>();
-    return R == 2 ? header_bytes_v3<512, 2>() : header_bytes_v3<512, 4>();
+    if (threads == 128) return R == 2 ? header_bytes_v3<128, 2>() : header_bytes_v3<128, 1>();
+    return R == 2 ? header_bytes_v3<256, 2>() : header_bytes_v3<256, 1>();
 }
 
 int max_smem_optin() {
@@ -862,20 +904,27 @@ int max_smem_optin() {
     return v;
 }
 
-// Column slice per CTA (THREADS * 16): 4096 by default (256 threads, two CTAs
-// per SM); the environment variable FUGAL_SWEEP_SLICE (2048, 4096 or 8192)
-// overrides it, trading cluster size against threads per CTA.
-int max_slice() {
+// Column slice per CTA (threads x columns per thread): 8192 (256 x 32) by
+// default above 4096 columns; the environment variable FUGAL_SWEEP_SLICE=4096
+// selects 256 x 16 (twice the cluster size, two rows per batch) instead.
+int slice_choice() {
     const char* e = getenv("FUGAL_SWEEP_SLICE");
-    const int v = e ? atoi(e) : 4096;
-    return (v == 2048 || v == 8192) ? v : 4096;
+    return (e && atoi(e) == 4096) ? 4096 : 8192;
 }
 
-// Launch shape for n columns: threads per CTA and CTAs per cluster, so that
-// cluster * threads * 16 >= n with the smallest power-of-two cluster.
-fugal_status plan_shape(int64_t n, int& threads, int& cluster) {
-    const int slice = n <= 2048 ? 2048 : max_slice();
-    threads = slice / kKPT;
+// Launch shape for n columns: threads per CTA, columns per thread, CTAs per
+// cluster (the smallest power of two covering n).
+fugal_status plan_shape(int64_t n, int& threads, int& kpt, int& cluster) {
+    if (n <= 2048) {
+        threads = 128; kpt = 16;
+    } else if (n <= 4096) {
+        threads = 128; kpt = 32;
+    } else if (slice_choice() == 4096) {
+        threads = 256; kpt = 16;
+    } else {
+        threads = 256; kpt = 32;
+    }
+    const int slice = threads * kpt;
     cluster = 1;
     while (static_cast<int64_t>(cluster) * slice < n) cluster <<= 1;
     if (cluster > kMaxCluster)
@@ -889,21 +938,21 @@ fugal_status plan_shape(int64_t n, int& threads, int& cluster) {
 constexpr int kSmemTarget = 100 * 1024;
 
 fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_occupancy) {
-    FUGAL_TRY(plan_shape(n, pl.threads, pl.cluster));
+    FUGAL_TRY(plan_shape(n, pl.threads, pl.kpt, pl.cluster));
     const int es = (kind != 0) ? 4 : elem_size(dt);
-    pl.R = rows_per_batch(es, pl.threads);
-    pl.slice_w = pl.threads * kKPT;
+    pl.R = rows_per_batch(pl.kpt);
+    pl.slice_w = pl.threads * pl.kpt;
     const size_t stage_bytes = static_cast<size_t>(pl.R) * pl.slice_w * es;
     const int sms = sm_count();
-    const int ctas_per_sm = pl.threads >= 512 ? 1 : 2;
+    const int ctas_per_sm = 2;
     // clusters the grid is expected to hold; the row-dual staging is sized from it
     int est = std::max(1, (sms * ctas_per_sm / pl.cluster) * 3 / 4);
-    KernelFn fn = kernel_for(pl.threads, dt, kind);
+    KernelFn fn = kernel_for(pl.threads, pl.kpt, dt, kind);
     for (int attempt = 0; attempt < 3; ++attempt) {
         pl.rows_pad = static_cast<int>(((n + est - 1) / est + 31) / 32 * 32);
         const size_t fixed = header_for(pl.threads, pl.R) + static_cast<size_t>(pl.slice_w) * 4 +
                              static_cast<size_t>(pl.rows_pad) * 4;
-        const int budget = pl.threads >= 512 ? max_smem_optin() : kSmemTarget;
+        const int budget = kSmemTarget;
         int stages = static_cast<int>((budget - static_cast<int64_t>(fixed)) / static_cast<int64_t>(stage_bytes));
         stages = std::min(stages, kMaxStages);
         if (stages < 2) stages = std::min(2, static_cast<int>((max_smem_optin() - static_cast<int64_t>(fixed)) /
@@ -1028,8 +1077,8 @@ extern "C" fugal_status fugal_sinkhorn_workspace_size(int64_t n, int stream_dtyp
     if (n <= 0) return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_workspace_size: n must be positive");
     if (stream_dtype < FUGAL_F32 || stream_dtype > FUGAL_F16)
         return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_workspace_size: bad stream dtype");
-    int threads, cluster;
-    FUGAL_TRY(plan_shape(n, threads, cluster));
+    int threads, kpt, cluster;
+    FUGAL_TRY(plan_shape(n, threads, kpt, cluster));
     *bytes = layout(n, nullptr, partial_rows_bound(n)).bytes;
     return FUGAL_OK;
 }
@@ -1167,7 +1216,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         const bool absorb = use16 && t >= p.fp32_warmup_sweeps && (t - p.fp32_warmup_sweeps) % p.reabsorb_every == 0;
         if (!use16 || t < p.fp32_warmup_sweeps) {
             SweepArgs a = sweep_args(plan32, p.cost32, p.ld32, nullptr, nullptr);
-            status = launch_sweep(plan32, kernel_for(plan32.threads, FUGAL_F32, 0), a, stream, FUGAL_KERNEL_SWEEP_F32);
+            status = launch_sweep(plan32, kernel_for(plan32.threads, plan32.kpt, FUGAL_F32, 0), a, stream, FUGAL_KERNEL_SWEEP_F32);
             if (status == FUGAL_OK) status = finalize(plan32.clusters);
         } else if (absorb) {
             // reads cost32 in the FP32 frame (offsets of the previous snapshot if any), writes snapshot snap_idx
@@ -1178,12 +1227,12 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
             a.ld16 = p.ld16;
             a.a_snap = w.a_snap + (snap_idx & 1) * w.n_pad;
             a.b_snap = w.b_snap + (snap_idx & 1) * w.n_pad;
-            status = launch_sweep(plan_abs, kernel_for(plan_abs.threads, FUGAL_F32, p.stream_dtype == FUGAL_BF16 ? 1 : 2),
+            status = launch_sweep(plan_abs, kernel_for(plan_abs.threads, plan_abs.kpt, FUGAL_F32, p.stream_dtype == FUGAL_BF16 ? 1 : 2),
                                   a, stream, FUGAL_KERNEL_ABSORB);
             if (status == FUGAL_OK) status = finalize(plan_abs.clusters);
         } else {
             SweepArgs a = sweep_args(plan16, p.cost16, p.ld16, nullptr, nullptr);
-            status = launch_sweep(plan16, kernel_for(plan16.threads, p.stream_dtype, 0), a, stream, FUGAL_KERNEL_SWEEP);
+            status = launch_sweep(plan16, kernel_for(plan16.threads, plan16.kpt, p.stream_dtype, 0), a, stream, FUGAL_KERNEL_SWEEP);
             if (status == FUGAL_OK) status = finalize(plan16.clusters);
         }
         if (status != FUGAL_OK) break;
@@ -1220,7 +1269,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         }
         for (int k = 0; k < p.polish_sweeps && status == FUGAL_OK; ++k) {
             SweepArgs a = sweep_args(plan32, p.cost32, p.ld32, nullptr, nullptr);
-            status = launch_sweep(plan32, kernel_for(plan32.threads, FUGAL_F32, 0), a, stream, FUGAL_KERNEL_SWEEP_F32);
+            status = launch_sweep(plan32, kernel_for(plan32.threads, plan32.kpt, FUGAL_F32, 0), a, stream, FUGAL_KERNEL_SWEEP_F32);
             if (status == FUGAL_OK) status = finalize(plan32.clusters);
         }
     }
