@@ -41,6 +41,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -295,7 +296,6 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     const int col0 = rank * p.slice_w;
     const int ncopy = max(0, min(p.slice_w, p.n_copy - col0));
     const int nvalid = max(0, min(p.slice_w, n - col0));
-    const bool full_slice = nvalid == p.slice_w;  // uniform per CTA: no column masking needed
     const int row_begin = cid * p.rows_per_cluster;
     const int row_end = min(n, row_begin + p.rows_per_cluster);
     const int nbatch = row_end > row_begin ? (row_end - row_begin + R - 1) / R : 0;
@@ -325,7 +325,18 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                 }
             }
         }
-        b_s[j] = b * kLog2e;
+        // columns past n contribute 2^(-inf) = 0 without any masking in the hot loop
+        b_s[j] = j < nvalid ? b * kLog2e : -INFINITY;
+    }
+    // Stage columns [ncopy, slice_w) are never written by the bulk copies: zero
+    // them once so that they hold finite values (their b_s is -inf).
+    if (ncopy < p.slice_w) {
+        const int tail = p.slice_w - ncopy;
+        for (int s = 0; s < p.stages; ++s)
+            for (int r = 0; r < R; ++r) {
+                T* row = reinterpret_cast<T*>(stage_base + s * stage_bytes) + static_cast<size_t>(r) * p.slice_w;
+                for (int j = tid; j < tail; j += THREADS) row[ncopy + j] = from_float<T>(0.f);
+            }
     }
     // Row duals of the previous sweep (the fast path's exponent reference and
     // the momentum term), read once here instead of on every batch's critical path.
@@ -434,11 +445,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                                          v2);
 #pragma unroll
                         for (int q = 0; q < VP; ++q) {
-                            float2 y = ex2_pair(__ffma2_rn(v2[q], log2e2, __fadd2_rn(b2[q], ref2[r])));
-                            if (!full_slice) {
-                                if (c + 2 * q >= nvalid) y.x = 0.f;
-                                if (c + 2 * q + 1 >= nvalid) y.y = 0.f;
-                            }
+                            const float2 y = ex2_pair(__ffma2_rn(v2[q], log2e2, __fadd2_rn(b2[q], ref2[r])));
                             e[r][g * VP + q] = y;
                             s2[r] = __fadd2_rn(s2[r], y);
                         }
@@ -489,9 +496,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                                          v2);
 #pragma unroll
                         for (int q = 0; q < VP; ++q) {
-                            float2 x = __ffma2_rn(v2[q], log2e2, b2[q]);
-                            if (c + 2 * q >= nvalid) x.x = -INFINITY;
-                            if (c + 2 * q + 1 >= nvalid) x.y = -INFINITY;
+                            const float2 x = __ffma2_rn(v2[q], log2e2, b2[q]);
                             e[r][g * VP + q] = x;
                             mx[r] = fmaxf(mx[r], fmaxf(x.x, x.y));
                         }
@@ -915,7 +920,13 @@ int slice_choice() {
 // Launch shape for n columns: threads per CTA, columns per thread, CTAs per
 // cluster (the smallest power of two covering n).
 fugal_status plan_shape(int64_t n, int& threads, int& kpt, int& cluster) {
-    if (n <= 2048) {
+    // FUGAL_SWEEP_SHAPE="threads,kpt" (threads 128 or 256, kpt 16 or 32) overrides the choice
+    const char* shape = getenv("FUGAL_SWEEP_SHAPE");
+    int st = 0, sk = 0;
+    if (shape != nullptr && sscanf(shape, "%d,%d", &st, &sk) == 2 && (st == 128 || st == 256) &&
+        (sk == 16 || sk == 32)) {
+        threads = st; kpt = sk;
+    } else if (n <= 2048) {
         threads = 128; kpt = 16;
     } else if (n <= 4096) {
         threads = 128; kpt = 32;

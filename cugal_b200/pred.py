@@ -68,7 +68,8 @@ class FrankWolfeEngine:
         self.ld = padded_ld(n)
         self.P_buf = torch.zeros((n, self.ld), dtype=torch.float32, device=dev)
         self.P_buf[:, :n] = 1.0 / n
-        self.cost32 = torch.empty((n, self.ld), dtype=torch.float32, device=dev)
+        # padding columns [n, ld) stay zero: the sweeps need them finite
+        self.cost32 = torch.zeros((n, self.ld), dtype=torch.float32, device=dev)
         self.U = torch.zeros(n, dtype=torch.float64, device=dev)
         self.V = torch.zeros(n, dtype=torch.float64, device=dev)
         self.u = torch.zeros(n, dtype=torch.float32, device=dev)

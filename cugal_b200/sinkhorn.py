@@ -45,7 +45,7 @@ class SinkhornSolver:
         self.ld16 = padded_ld(n)
         self.cost16 = None
         if self.stream_dtype != N.FUGAL_F32:
-            self.cost16 = torch.empty((n, self.ld16), dtype=config.stream_dtype, device=self.device)
+            self.cost16 = torch.zeros((n, self.ld16), dtype=config.stream_dtype, device=self.device)
 
     def params(self, cost32: torch.Tensor, u_out: torch.Tensor, v_out: torch.Tensor, record_ptr: int | None):
         c = self.config
@@ -119,7 +119,7 @@ class SinkhornState:
         n = self.n
         N.require_cuda(C, "C")
         K = (-C / config.sinkhorn_regularization).to(torch.float32)
-        cost32 = torch.empty((n, padded_ld(n)), dtype=torch.float32, device=C.device)
+        cost32 = torch.zeros((n, padded_ld(n)), dtype=torch.float32, device=C.device)  # finite padding
         cost32[:, :n] = (K.double() + self.U[:, None] + self.V[None, :]).float()
         self._solver.solve(cost32, self._du, self._dv, self._rec.data_ptr())
         self.U += self._du.double()

@@ -181,7 +181,8 @@ fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointers, const i
  * switches, after fp32_warmup_sweeps, to the reduced-precision copy `cost16`
  * (which it writes, refreshed every reabsorb_every sweeps), then runs
  * polish_sweeps FP32 sweeps.  Outputs: u_out / v_out (FP32, n) in the frame of
- * cost32, and an optional DEVICE fugal_solve_record. */
+ * cost32, and an optional DEVICE fugal_solve_record.  Padding columns [n, ld)
+ * of cost32 and cost16 must hold finite values (zero them once). */
 typedef struct {
     int64_t n;
     const float* cost32;

@@ -87,10 +87,14 @@ def _plan(C, u, v, reg):
     return np.exp(-C / reg + u[:, None] + v[None, :])
 
 
-@pytest.mark.parametrize("n,slice_w", [(64, None), (300, None), (3000, None), (3000, "2048"), (5000, "2048")])
-def test_sinkhorn_fp32_matches_oracle(n, slice_w, monkeypatch):
-    if slice_w:
-        monkeypatch.setenv("FUGAL_SWEEP_SLICE", slice_w)  # forces 2- and 4-CTA clusters
+# Launch shapes: n <= 2048 -> 128 threads x 16 columns, <= 4096 -> 128 x 32, else 256 x 32 with
+# clusters of ceil(n / 8192) CTAs; FUGAL_SWEEP_SHAPE overrides.  Sizes are picked so that some
+# CTA's slice has chunk-columns entirely past n (64, 500, 4104 and 8200 do).
+@pytest.mark.parametrize("n,shape", [(64, None), (300, None), (500, None), (3000, None), (3000, "128,16"),
+                                     (4104, "256,16"), (5000, None), (5000, "256,16")])
+def test_sinkhorn_fp32_matches_oracle(n, shape, monkeypatch):
+    if shape:
+        monkeypatch.setenv("FUGAL_SWEEP_SHAPE", shape)
     rng = np.random.default_rng(n)
     C = rng.random((n, n)) * 4
     C = C.astype(np.float32).astype(np.float64)
@@ -119,14 +123,16 @@ def test_sinkhorn_fp32_matches_oracle(n, slice_w, monkeypatch):
     np.testing.assert_allclose(_plan(C2, u2, v2, reg), _plan(C2, ref2.u, ref2.v, reg), atol=1e-4)
 
 
-def test_sinkhorn_two_cta_cluster_512_threads():
-    n = 9000  # 512 threads per CTA, 2-CTA clusters
+@pytest.mark.parametrize("n", [8200, 9000])
+def test_sinkhorn_two_cta_cluster(n):
+    # 256 threads x 32 columns per CTA, 2-CTA clusters; the second slice holds 8 / 808 columns
     rng = np.random.default_rng(9)
     C = (rng.random((n, n)) * 4).astype(np.float32).astype(np.float64)
     zero = np.zeros(n)
     ref = O.sinkhorn_log_solve(C, zero, zero, 0.05, 8, 0.0, 10)
     u, v, prof = _solve_gpu(C, zero, zero, 0.05, 8, 0.0, 10)
     assert prof.iteration_count == 8
+    np.testing.assert_allclose(u, ref.u, atol=1e-4)
     np.testing.assert_allclose(_plan(C, u, v, 0.05), _plan(C, ref.u, ref.v, 0.05), atol=1e-4)
 
 
