@@ -129,25 +129,26 @@ FUGAL_DEVICE void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
-// Non-blocking probe of phase `parity`; true once that phase has completed.
-FUGAL_DEVICE bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+// Probe of phase `parity`: true once that phase has completed.  The thread may
+// be suspended for up to `hint_ns` while the phase is pending.
+FUGAL_DEVICE bool mbar_try_wait(uint64_t* bar, uint32_t parity, uint32_t hint_ns = kSuspendHintNs) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n"
         " mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n"
         " selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendHintNs)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
 // Bounded wait: returns false (and records FUGAL_DEVICE_TIMEOUT) if the phase
 // does not complete within kWaitLimitNs.
-FUGAL_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    if (mbar_try_wait(bar, parity)) return true;
+FUGAL_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, uint32_t hint_ns = kSuspendHintNs) {
+    if (mbar_try_wait(bar, parity, hint_ns)) return true;
     const uint64_t t0 = global_timer_ns();
     for (uint32_t i = 0; i < kMaxPolls; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait(bar, parity, hint_ns)) return true;
         if (global_timer_ns() - t0 > kWaitLimitNs) break;
     }
     report_error(err, FUGAL_DEVICE_TIMEOUT);

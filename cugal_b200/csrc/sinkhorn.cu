@@ -140,6 +140,7 @@ struct SweepArgs {
     int slice_w;          // columns per CTA = threads x columns per thread
     int rows_per_cluster;
     int rows_pad;         // rows_per_cluster rounded up to 32 (shared staging of the row duals)
+    unsigned suspend_ns;  // mbarrier try_wait suspend-time hint of the sweep's waits
     int stages;
     const float* b_buf;   // [2][n_pad] column duals of consecutive sweeps
     const float* b_off;   // frame offset added to the previous b (nullable)
@@ -203,7 +204,7 @@ __host__ __device__ constexpr int header_bytes_v3() {
 // Returns the slot to read, or -1 if the wait timed out.
 template <int THREADS, int R>
 __device__ __forceinline__ int exchange(float2* xch, uint64_t* xbar, int C, int rank, int& xuse, const float* m,
-                                        const float* sm, int* err) {
+                                        const float* sm, int* err, unsigned hint_ns) {
     constexpr int WARPS = THREADS / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int slot = xuse & 1;
@@ -217,7 +218,7 @@ __device__ __forceinline__ int exchange(float2* xch, uint64_t* xbar, int C, int 
             st_async_f32x2(map_to_rank(&xch[((slot * kMaxCluster + rank) * WARPS + warp) * R + r], lane), m[r], sm[r],
                            bar);
     }
-    return mbar_wait(&xbar[slot], parity, err) ? slot : -1;
+    return mbar_wait(&xbar[slot], parity, err, hint_ns) ? slot : -1;
 }
 
 // Reductions over the C x WARPS partials of one row held in slot `slot`: every
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     int bt = 0;
     for (; bt < nbatch; ++bt) {
         const int s = bt % p.stages;
-        if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status))) {
+        if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status, p.suspend_ns))) {
             alive = false;
             break;
         }
@@ -425,11 +426,12 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
             // ---- fast path: exponents relative to the previous row normaliser -a_old:
             //      e = 2^(L log2e + b2 + a_old log2e)
             float sm[R], zero[R];
-            float2 s2[R], ref2[R];
+            float2 s2[R], t2[R], ref2[R];  // two partial sums per row (even / odd pairs) for ILP
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 ref2[r] = make_float2(a_old[r] * kLog2e, a_old[r] * kLog2e);
                 s2[r] = make_float2(0.f, 0.f);
+                t2[r] = make_float2(0.f, 0.f);
                 zero[r] = 0.f;
             }
 #pragma unroll
@@ -447,14 +449,20 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                         for (int q = 0; q < VP; ++q) {
                             const float2 y = ex2_pair(__ffma2_rn(v2[q], log2e2, __fadd2_rn(b2[q], ref2[r])));
                             e[r][g * VP + q] = y;
-                            s2[r] = __fadd2_rn(s2[r], y);
+                            if (q & 1)
+                                t2[r] = __fadd2_rn(t2[r], y);
+                            else
+                                s2[r] = __fadd2_rn(s2[r], y);
                         }
                     }
                 }
             }
 #pragma unroll
-            for (int r = 0; r < R; ++r) sm[r] = warp_sum(s2[r].x + s2[r].y);
-            const int slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status);
+            for (int r = 0; r < R; ++r) {
+                const float2 u2 = __fadd2_rn(s2[r], t2[r]);
+                sm[r] = warp_sum(u2.x + u2.y);
+            }
+            const int slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status, p.suspend_ns);
             if (!agree(slot >= 0)) {
                 alive = false;
                 break;
@@ -508,7 +516,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) mx[r] = warp_max(mx[r]);
-            int slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, mx, zero, &st->status);
+            int slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, mx, zero, &st->status, p.suspend_ns);
             if (!agree(slot >= 0)) {
                 alive = false;
                 break;
@@ -529,7 +537,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                 }
                 sm[r] = warp_sum(ss.x + ss.y);
             }
-            slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status);
+            slot = exchange<THREADS, R>(xch, xbar, C, rank, xuse, zero, sm, &st->status, p.suspend_ns);
             if (!agree(slot >= 0)) {
                 alive = false;
                 break;
@@ -870,6 +878,15 @@ int elem_size(int dt) { return dt == FUGAL_F32 ? 4 : 2; }
 
 using KernelFn = void (*)(const SweepArgs);
 
+// mbarrier try_wait suspend-time hint for the sweep's waits, in ns
+// (FUGAL_SUSPEND_NS overrides the default).
+unsigned suspend_hint() {
+    const char* e = getenv("FUGAL_SUSPEND_NS");
+    if (e == nullptr) return kSuspendHintNs;
+    const long v = atol(e);
+    return static_cast<unsigned>(v < 0 ? 0 : (v > 1000000 ? 1000000 : v));
+}
+
 // Launch shapes: (threads per CTA, columns per thread).  Rows per batch are
 // 32 / columns-per-thread, so a thread always holds 32 exponentials.
 constexpr int rows_per_batch(int kpt) { return 32 / kpt; }
@@ -1183,6 +1200,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         a.slice_w = pl.slice_w;
         a.rows_per_cluster = pl.rows_per_cluster;
         a.rows_pad = pl.rows_pad;
+        a.suspend_ns = suspend_hint();
         a.stages = pl.stages;
         a.b_buf = w.b_buf;
         a.b_buf_w = w.b_buf;
