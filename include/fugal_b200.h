@@ -171,6 +171,28 @@ fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointers, const i
                                double out_scale, const double* U, const double* V, float* out, int64_t ldo,
                                void* workspace, size_t workspace_bytes, fugal_stream_t stream);
 
+/* No counterpart in the reference.  fugal_fw_gradient for callers that cannot
+ * allocate device memory (a host whose device memory belongs to a pool allocator
+ * every allocation must go through, or a binding that only passes input and
+ * output pointers): same arguments and result, minus the workspace, which comes
+ * from one FUGAL_FIXED_SCRATCH_BYTES array compiled into the library.  Every GPU
+ * on which the library's device code is loaded holds that array until the
+ * process exits.  n above FUGAL_FIXED_SCRATCH_MAX_N is rejected with
+ * FUGAL_BAD_SHAPE.  The call allocates nothing.  Its first call on a device (that
+ * device current) looks up the array's device address; make that first call
+ * before any stream capture.  All calls on a device share the array and it keeps
+ * the last call's contents (nothing in it needs to start at zero); calls whose
+ * kernels overlap on the GPU race on it, so order them on one stream. */
+#define FUGAL_FIXED_SCRATCH_BYTES (16 * 1024 * 1024)
+#define FUGAL_FIXED_SCRATCH_MAX_N 2048
+fugal_status fugal_fw_gradient_fixed_scratch(int64_t n, const int32_t* a_row_pointers,
+                                             const int32_t* a_col_indices, const int32_t* b_row_pointers,
+                                             const int32_t* b_col_indices, const float* P, int64_t ldp,
+                                             const float* source_features, const float* target_features,
+                                             const float* D, int64_t ldd, double lambda, double lambda_scale,
+                                             double out_scale, const double* U, const double* V, float* out,
+                                             int64_t ldo, fugal_stream_t stream);
+
 /* Log-domain Sinkhorn solve (cugal/sinkhorn.py:90-120) on the absorbed cost
  * cost32 = K + U_i + V_j, warm-started at u = v = 0 relative to that frame.
  * Same iteration as the reference: per iteration a column then a row update
