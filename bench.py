@@ -59,6 +59,8 @@ def parse_args(argv=None):
     ap.add_argument("--sinkhorn-iterations", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp32-warmup-sweeps", type=int, default=None, help="override Config.fp32_warmup_sweeps")
+    ap.add_argument("--reabsorb-every", type=int, default=None, help="override Config.reabsorb_every")
     return ap.parse_args(argv)
 
 
@@ -187,6 +189,25 @@ def traffic_per_launch(n: int, ld: int):
     return d["dram_bytes_per_launch"] * (n * ld) / (d["n"] * d["ld"])
 
 
+def executed_sweeps(iteration_counts, config) -> dict:
+    """Sweeps per kernel family that did their work, from each solve's iteration
+    count and the solve schedule (FP32 warm-up sweeps, an absorb sweep every
+    reabsorb_every sweeps after them, 16-bit sweeps, FP32 polish sweeps).  Sweeps
+    launched after convergence return at once and are not counted here."""
+    out = {"sweep16": 0, "sweep32": 0, "absorb": 0}
+    for its in iteration_counts:
+        if config.stream_dtype is None:
+            out["sweep32"] += its
+            continue
+        warm = min(its, config.fp32_warmup_sweeps)
+        out["sweep32"] += warm + config.polish_sweeps
+        rest = its - warm
+        absorbs = (rest + config.reabsorb_every - 1) // config.reabsorb_every
+        out["absorb"] += absorbs
+        out["sweep16"] += rest - absorbs
+    return out
+
+
 def reference_gpu_sample(n: int, solves: int, sweeps: float, iters: int = 20):
     """Seconds per alignment of the reference's FP32 GPU Sinkhorn (its own kernels,
     oracle/_ref), extrapolated from `iters` timed iterations at size n, or None."""
@@ -257,6 +278,10 @@ def run_ours(args):
         over["iter_count"] = args.iter_count
     if args.sinkhorn_iterations:
         over["sinkhorn_iterations"] = args.sinkhorn_iterations
+    if args.fp32_warmup_sweeps is not None:
+        over["fp32_warmup_sweeps"] = args.fp32_warmup_sweeps
+    if args.reabsorb_every is not None:
+        over["reabsorb_every"] = args.reabsorb_every
     config = config_for(w, **over)
     n = src.number_of_nodes()
     A = Adjacency.from_graph(src, config.device)
@@ -291,9 +316,14 @@ def run_ours(args):
     fam = {name: N.timing_query(k) for k, name in enumerate(N.KERNEL_FAMILY_NAMES)}
     cols_np = cols.cpu().numpy() if isinstance(cols, torch.Tensor) else np.asarray(cols)
     accuracy = float(np.mean(cols_np == perm))
-    profiles[-1].resolve()
+    for p in profiles:
+        p.resolve()
     sk = [p.iteration_count for p in profiles[-1].sinkhorn_profiles]
     mean_sweeps = float(np.mean(sk)) if sk else 0.0
+    fe = np.array([p.final_error for p in profiles[-1].sinkhorn_profiles], dtype=np.float64)
+    final_err = {"median": float(np.median(fe)), "max": float(np.max(fe)),
+                 "above_threshold": int(np.sum(fe >= config.sinkhorn_threshold)),
+                 "threshold": config.sinkhorn_threshold, "solves": int(fe.size)} if fe.size else None
 
     # end-to-end through cugal() from host graphs
     import networkx as nx
@@ -317,9 +347,12 @@ def run_ours(args):
     peak, peak_kind = load_peak()
     fam_key = "sweep16" if sdt is not None else "sweep32"
     nl, ms = fam[fam_key]
+    all_solves = [c for p in profiles for c in (q.iteration_count for q in p.sinkhorn_profiles)]
+    real = executed_sweeps(all_solves, config)[fam_key]
     elem = 2 if sdt is not None else 4
     bytes_per = n * ld * elem
-    achieved = bytes_per / (ms / nl / 1e3) / 1e9 if nl else None
+    # time of every launch of the family (the few that return at once included) over the sweeps that ran
+    achieved = bytes_per * real / (ms / 1e3) / 1e9 if real else None
     traffic = traffic_per_launch(n, ld) if sdt is not None else None
 
     cpu = None
@@ -348,14 +381,16 @@ def run_ours(args):
                        "edges_target": tgt.number_of_edges(), "stream_dtype": args.stream_dtype,
                        "fw_steps": config.iter_count * config.frank_wolfe_iter_count,
                        "sinkhorn_iterations": config.sinkhorn_iterations, "reg": config.sinkhorn_regularization,
+                       "fp32_warmup_sweeps": config.fp32_warmup_sweeps, "reabsorb_every": config.reabsorb_every,
+                       "polish_sweeps": config.polish_sweeps,
                        "lap": config.hungarian_method.value, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (cost copy n*ld*2 bytes)"},
             "node_accuracy": accuracy, "e2e_node_accuracy": e2e_acc,
-            "mean_sinkhorn_iterations": mean_sweeps,
+            "mean_sinkhorn_iterations": mean_sweeps, "sinkhorn_final_error": final_err,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "kernel": f"sweep_kernel<{args.stream_dtype}>", "launches": nl,
-                         "avg_launch_ms": ms / nl if nl else None, "bytes_per_launch": bytes_per,
+                         "kernel": f"sweep_kernel<{args.stream_dtype}>", "launches": nl, "sweeps_run": real,
+                         "avg_launch_ms": ms / real if real else None, "bytes_per_launch": bytes_per,
                          "peak_kind": peak_kind, "launch_shape": plan},
             "kernel_times_ms": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in fam.items()},
             "cpu_baseline": cpu,

@@ -1091,6 +1091,10 @@ fugal_status launch_sweep(const SweepPlan& pl, KernelFn fn, const SweepArgs& arg
 // every solve takes two fresh slots so a late copy of an earlier solve on
 // another stream cannot be mistaken for this one's.
 constexpr int kPinnedSlots = 64;
+// The host reads the flag copied at an evaluation point kPollLag sweeps later:
+// the stream still holds that many sweeps of work while the host waits, and at
+// most kPollLag sweeps (which return at once) are launched after convergence.
+constexpr int kPollLag = 2;
 thread_local int* g_pinned_ring = nullptr;
 thread_local int g_pinned_next = 0;
 
@@ -1238,8 +1242,15 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         cudaEventDestroy(ev[1]);
     };
     int slot = 0;
-    bool pending[2] = {false, false};
+    int poll_slot = -1, poll_t = 0;  // the copy of `done` in flight, issued after sweep poll_t
     fugal_status status = FUGAL_OK;
+    auto read_poll = [&](bool& stop) -> fugal_status {
+        const fugal_status s = cuda_check(cudaEventSynchronize(ev[poll_slot]), "sinkhorn: poll wait");
+        timing_poll();
+        stop = s == FUGAL_OK && g_pinned_done[poll_slot] != 0;
+        poll_slot = -1;
+        return s;
+    };
     for (int t = 0; t < p.max_iterations && status == FUGAL_OK; ++t) {
         const int snap_idx = (!use16 || t < p.fp32_warmup_sweeps) ? -1 : ((t - p.fp32_warmup_sweeps) / p.reabsorb_every);
         const bool absorb = use16 && t >= p.fp32_warmup_sweeps && (t - p.fp32_warmup_sweeps) % p.reabsorb_every == 0;
@@ -1265,21 +1276,24 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
             if (status == FUGAL_OK) status = finalize(plan16.clusters);
         }
         if (status != FUGAL_OK) break;
+        bool stop = false;
+        if (poll_slot >= 0 && t - poll_t >= kPollLag) {
+            status = read_poll(stop);
+            if (status != FUGAL_OK || stop) break;
+        }
         const bool eval_point = (t % p.eval_freq == 0 && t != 0);
         if (eval_point) {
+            if (poll_slot >= 0) {  // eval_freq < kPollLag: settle the older poll first
+                status = read_poll(stop);
+                if (status != FUGAL_OK || stop) break;
+            }
+            slot ^= 1;
             status = cuda_check(cudaMemcpyAsync(&g_pinned_done[slot], &w.st->done, sizeof(int),
                                                 cudaMemcpyDeviceToHost, stream),
                                 "sinkhorn: poll copy");
             if (status == FUGAL_OK) status = cuda_check(cudaEventRecord(ev[slot], stream), "sinkhorn: poll event");
-            pending[slot] = true;
-            const int other = slot ^ 1;
-            if (status == FUGAL_OK && pending[other]) {
-                status = cuda_check(cudaEventSynchronize(ev[other]), "sinkhorn: poll wait");
-                pending[other] = false;
-                timing_poll();
-                if (status == FUGAL_OK && g_pinned_done[other]) break;
-            }
-            slot = other;
+            poll_slot = slot;
+            poll_t = t;
         }
     }
     if (status != FUGAL_OK) {

@@ -50,7 +50,13 @@ template <bool VEC>
 __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const int* __restrict__ col,
                                              const float* __restrict__ X, long long ldx, int n, int row, int c,
                                              bool c_ok) {
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    // two packed FP32x2 accumulators (fadd.f32x2); each column still sums its
+    // neighbours one by one in CSR order
+    float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
+    auto add = [&](const float4& v) {
+        lo = __fadd2_rn(lo, make_float2(v.x, v.y));
+        hi = __fadd2_rn(hi, make_float2(v.z, v.w));
+    };
     const int lane = threadIdx.x & 31;
     const int rs = rp[row], re = rp[row + 1];
     for (int e = rs; e < re; e += 32) {
@@ -67,21 +73,18 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
                 const float4 v1 = load4<VEC>(X, ldx, k1, c, n);
                 const float4 v2 = load4<VEC>(X, ldx, k2, c, n);
                 const float4 v3 = load4<VEC>(X, ldx, k3, c, n);
-                acc.x += v0.x; acc.y += v0.y; acc.z += v0.z; acc.w += v0.w;
-                acc.x += v1.x; acc.y += v1.y; acc.z += v1.z; acc.w += v1.w;
-                acc.x += v2.x; acc.y += v2.y; acc.z += v2.z; acc.w += v2.w;
-                acc.x += v3.x; acc.y += v3.y; acc.z += v3.z; acc.w += v3.w;
+                add(v0);
+                add(v1);
+                add(v2);
+                add(v3);
             }
         }
         for (; q < cnt; ++q) {
             const int k = __shfl_sync(0xffffffffu, idx, q);
-            if (c_ok) {
-                const float4 v = load4<VEC>(X, ldx, k, c, n);
-                acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
-            }
+            if (c_ok) add(load4<VEC>(X, ldx, k, c, n));
         }
     }
-    return acc;
+    return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
 
 // Fill tile[r][0..127] with the gathered rows r0 .. r0+31 of A X for columns c0 .. c0+127.
@@ -173,22 +176,27 @@ __global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __res
     if (j >= n) return;
     const double vj = ep.V ? ep.V[j] : 0.0;
     const float4 f2 = has_f ? fj[lane] : make_float4(0, 0, 0, 0);
+    const float lam = static_cast<float>(ep.lam);
     for (int ii = warp; ii < kTileCols; ii += kSpmmThreads / 32) {
         const int i = i0 + ii;
         if (i >= n) break;
-        const double apb = static_cast<double>(tile[lane][ii]);
-        const double p = static_cast<double>(ep.P[static_cast<size_t>(i) * ep.ldp + j]);
-        double g = -2.0 * apb + ep.lam * (1.0 - 2.0 * p);
+        // The gradient itself in FP32, as the reference computes it (SpMM, distance,
+        // regularize: cugal/pred.py:54-74, distance.cu:11-53, regularize.cu:10-39) ...
+        const float apb = tile[lane][ii];
+        const float p = ep.P[static_cast<size_t>(i) * ep.ldp + j];
+        float g = __fadd_rn(__fmul_rn(-2.0f, apb), __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, p))));
         if (has_f) {
             const float4 f1 = fi[ii];
-            const double d0 = (double)f1.x - (double)f2.x, d1 = (double)f1.y - (double)f2.y;
-            const double d2 = (double)f1.z - (double)f2.z, d3 = (double)f1.w - (double)f2.w;
-            g += sqrt(d0 * d0 + d1 * d1 + d2 * d2 + d3 * d3);
+            const float d0 = __fsub_rn(f1.x, f2.x), d1 = __fsub_rn(f1.y, f2.y);
+            const float d2 = __fsub_rn(f1.z, f2.z), d3 = __fsub_rn(f1.w, f2.w);
+            g = __fadd_rn(g, __fsqrt_rn(__fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))))));
         } else if (ep.D != nullptr) {
-            g += static_cast<double>(ep.D[static_cast<size_t>(i) * ep.ldd + j]);
+            g = __fadd_rn(g, ep.D[static_cast<size_t>(i) * ep.ldd + j]);
         }
+        // ... and its combination with the accumulated duals in FP64: the terms are
+        // O(1/reg) and cancel to O(1), which FP32 would not resolve.
         const double ui = ep.U ? ep.U[i] : 0.0;
-        ep.out[static_cast<size_t>(i) * ep.ldo + j] = static_cast<float>(ep.out_scale * g + ui + vj);
+        ep.out[static_cast<size_t>(i) * ep.ldo + j] = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + vj));
     }
 }
 

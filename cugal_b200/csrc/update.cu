@@ -26,6 +26,9 @@ inline dim3 ew_grid(int64_t n) {
 }
 
 // q = exp(L + u_i + v_j); P += alpha (q - P); gap += (q - P) * (-reg (L - U_i - V_j)).
+// Grid-stride over (row, 1024-column chunk) units, each thread one float4 of a
+// unit per step; every block reduces its gap once at the end (one FP64 atomic
+// per block instead of one per unit).
 __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict__ P, long long ldp,
                                                                const float* __restrict__ L, long long ldl,
                                                                const float* __restrict__ u,
@@ -34,10 +37,14 @@ __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict
                                                                const double* __restrict__ V, int n, float alpha,
                                                                double reg, double* gap) {
     __shared__ double red[32];
-    const int i = blockIdx.x;
-    const int j0 = (blockIdx.y * blockDim.x + threadIdx.x) * 4;
+    constexpr int kChunk = kEwThreads * 4;
+    const int chunks = (n + kChunk - 1) / kChunk;
+    const long long units = static_cast<long long>(n) * chunks;
     double g = 0.0;
-    if (j0 < n) {
+    for (long long w = blockIdx.x; w < units; w += gridDim.x) {
+        const int i = static_cast<int>(w / chunks);
+        const int j0 = static_cast<int>(w % chunks) * kChunk + threadIdx.x * 4;
+        if (j0 >= n) continue;
         const float ui = u[i];
         const double Ui = U ? U[i] : 0.0;
         float* prow = P + static_cast<size_t>(i) * ldp;
@@ -217,8 +224,10 @@ extern "C" fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const 
     FUGAL_TRY(cuda_check(cudaMemsetAsync(gap, 0, sizeof(double), stream), "fugal_fw_update: clear gap"));
     {
         LaunchScope scope(FUGAL_KERNEL_UPDATE, stream);
-        fw_update_kernel<<<ew_grid(n), kEwThreads, 0, stream>>>(P, ldp, cost32, ld32, u, v, U, V, static_cast<int>(n),
-                                                                 static_cast<float>(alpha), regularization, gap);
+        const int64_t units = n * ((n + kEwThreads * 4 - 1) / (kEwThreads * 4));
+        const int blocks = static_cast<int>(std::min<int64_t>(units, static_cast<int64_t>(sm_count()) * 8));
+        fw_update_kernel<<<blocks, kEwThreads, 0, stream>>>(P, ldp, cost32, ld32, u, v, U, V, static_cast<int>(n),
+                                                            static_cast<float>(alpha), regularization, gap);
         FUGAL_TRY(launch_check(who));
     }
     if (commit) {

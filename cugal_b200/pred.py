@@ -30,6 +30,7 @@ from . import _native as N
 from .adjacency import Adjacency
 from .config import Config, HungarianMethod, SinkhornMethod
 from .feature_extraction import Features
+from .exact_lap import FUGAL_ITER_LIMIT, FUGAL_OK, exact_assign
 from .greedy_lap import greedy_assign
 from .profile import Phase, Profile, SinkhornProfile, TimeStamp
 from .sinkhorn import SinkhornSolver, padded_ld, read_record
@@ -152,7 +153,13 @@ def round_on_device(P: torch.Tensor, config: Config, profile: Profile):
     start_time = TimeStamp(config.device)
     method = config.hungarian_method
     if method == HungarianMethod.SCIPY:
-        _, cols = scipy.optimize.linear_sum_assignment(P.cpu().numpy(), maximize=True)
+        cols, _, status = exact_assign(P, maximize=True)
+        st = int(status.item())
+        if st == FUGAL_ITER_LIMIT:
+            # the device search hit its step cap: scipy itself gives the same mapping
+            _, cols = scipy.optimize.linear_sum_assignment(P.cpu().numpy(), maximize=True)
+        elif st != FUGAL_OK:
+            raise N.NativeError(f"fugal_exact_lap: device status {st}")
     elif method in GREEDY_METHODS:
         cols = greedy_assign(P, method, config.lap_candidates)
     elif method == HungarianMethod.SPARSE:

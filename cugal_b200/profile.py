@@ -32,6 +32,9 @@ class SinkhornProfile:
     errors: list[float] = field(default_factory=list)
     iteration_count: int = 0
     time: float = 0.0
+    # column-marginal L1 error of the returned plan, measured in FP32 (after the
+    # polish sweeps when the solve streamed a reduced-precision cost)
+    final_error: float = float("nan")
 
     @staticmethod
     def average(profiles: list["SinkhornProfile"]) -> "SinkhornProfile":

@@ -83,7 +83,8 @@ def read_record(raw: torch.Tensor) -> SinkhornProfile:
     if rec.status != 0:
         raise N.NativeError(f"Sinkhorn solve reported device status {rec.status} (bounded wait timed out)")
     errors = [rec.errors[k] for k in range(rec.n_errors)]
-    return SinkhornProfile(errors=errors, iteration_count=rec.iteration_count)
+    final = rec.polish_error if rec.polish_count > 0 else rec.last_error
+    return SinkhornProfile(errors=errors, iteration_count=rec.iteration_count, final_error=final)
 
 
 class SinkhornState:

@@ -146,6 +146,20 @@ fugal_status fugal_greedy_lap(float* P, int64_t ldp, int64_t n, int method, cons
                               int candidates, int mutate, int64_t* columns_out, void* workspace,
                               size_t workspace_bytes, fugal_stream_t stream);
 
+/* Exact assignment with the same mapping as scipy.optimize.linear_sum_assignment
+ * (the reference's HungarianMethod.SCIPY rounding, cugal/pred.py:151-158): cost
+ * c = -P (maximize != 0) or P, converted to double; Crouse's shortest augmenting
+ * path with scipy's candidate order and tie rules, so ties resolve as scipy
+ * resolves them.  columns_out[r] = column of row r (int64, device).  The search
+ * stops after max_steps Dijkstra steps in total.  *status_out (device int32)
+ * receives FUGAL_OK, FUGAL_ITER_LIMIT (cap hit; columns_out not written),
+ * FUGAL_NONFINITE (NaN, or -inf cost) or FUGAL_BAD_ARGUMENT (infeasible);
+ * *steps_out (device int64, nullable) the steps taken. */
+fugal_status fugal_exact_lap_workspace_size(int64_t n, size_t* bytes);
+fugal_status fugal_exact_lap(const float* P, int64_t ldp, int64_t n, int maximize, int64_t max_steps,
+                             int64_t* columns_out, int64_t* steps_out, int32_t* status_out, void* workspace,
+                             size_t workspace_bytes, fugal_stream_t stream);
+
 /* count of entries of P (n x n) that are <= threshold (cugal/pred.py:152-153), into a DEVICE int64. */
 fugal_status fugal_count_le(const float* P, int64_t ldp, int64_t n, float threshold, int64_t* count,
                             fugal_stream_t stream);
@@ -155,7 +169,7 @@ fugal_status fugal_count_le(const float* P, int64_t ldp, int64_t n, float thresh
 /* Gradient with the Sinkhorn kernel matrix fused into its epilogue
  * (cugal/pred.py:54-74 sparse_gradient + add_feature_distance :30-35 +
  * regularize + K = -C/reg at cugal/sinkhorn.py:98), for symmetric A and B:
- *   C[i][j]   = -2 (A P B)[i][j] + ||Fs_i - Ft_j|| + lambda_scale * lambda * (1 - 2 P[i][j])
+ *   C[i][j]   = -2 (A P B)[i][j] + ||Fs_i - Ft_j|| + lambda_scale * lambda * (1 - 2 P[i][j])   (FP32)
  *   out[i][j] = out_scale * C[i][j] + U[i] + V[j]          (FP64 arithmetic, FP32 store)
  * out_scale = -1/reg with U, V the accumulated duals gives the absorbed Sinkhorn
  * input; out_scale = 1, U = V = NULL gives the plain gradient.  Features are the
