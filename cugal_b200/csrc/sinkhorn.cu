@@ -141,6 +141,7 @@ struct SweepArgs {
     int rows_per_cluster;
     int rows_pad;         // rows_per_cluster rounded up to 32 (shared staging of the row duals)
     unsigned suspend_ns;  // mbarrier try_wait suspend-time hint of the sweep's waits
+    int pipeline;         // 16-bit fast sweeps: stage exponentials in TMEM, overlap the exchanges
     int stages;
     const float* b_buf;   // [2][n_pad] column duals of consecutive sweeps
     const float* b_off;   // frame offset added to the previous b (nullable)
@@ -187,13 +188,14 @@ FUGAL_DEVICE float lanes_max(float v) {
 }
 
 // Shared-memory layout of the sweep kernel (byte offsets from the dynamic base):
-//   [0, 128)          mbarriers: full[kMaxStages] (stage loaded), xbar[2] (exchange done)
-//   [128, header)     xch[2][kMaxCluster][WARPS][R] float2: per-warp row partials of every CTA
+//   [0, 128)          mbarriers: full[kMaxStages] (stage loaded), xbar[kXSlots] (exchange done)
+//   [128, header)     xch[kXSlots][kMaxCluster][WARPS][R] float2: per-warp row partials of every CTA
 //   [header, +4 W)    b_s[slice_w]: this sweep's column duals for the CTA's slice
-//   then              stages[stages][R][slice_w] elements of the streamed cost
+//   then              a_s[rows_pad], stages[stages][R][slice_w] elements of the streamed cost
+constexpr int kXSlots = 4;
 template <int THREADS, int R>
 __host__ __device__ constexpr int header_bytes_v3() {
-    return ((kBarBytes + 2 * kMaxCluster * (THREADS / 32) * R * 8) + 127) / 128 * 128;
+    return ((kBarBytes + kXSlots * kMaxCluster * (THREADS / 32) * R * 8) + 127) / 128 * 128;
 }
 
 // One cluster-wide all-to-all of per-warp row partials.  Every warp sends its R
@@ -219,6 +221,29 @@ __device__ __forceinline__ int exchange(float2* xch, uint64_t* xbar, int C, int 
                            bar);
     }
     return mbar_wait(&xbar[slot], parity, err, hint_ns) ? slot : -1;
+}
+
+// Split form of the exchange for the pipelined sweep: exchange number `xi` uses
+// slot xi % kXSlots.  Every CTA reads the data of exchange j before it sends
+// exchange j + 2 and sends exchange k only after exchange k - 2 has completed,
+// so with four slots a slot is never overwritten while a peer still reads it.
+template <int THREADS, int R>
+__device__ __forceinline__ void xsend(float2* xch, uint64_t* xbar, int C, int rank, int xi, const float* m,
+                                      const float* sm) {
+    constexpr int WARPS = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = xi % kXSlots;
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&xbar[slot], static_cast<uint32_t>(C * WARPS * R * 8));
+    if (lane < C) {
+        const uint32_t bar = map_to_rank(&xbar[slot], lane);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            st_async_f32x2(map_to_rank(&xch[((slot * kMaxCluster + rank) * WARPS + warp) * R + r], lane), m[r], sm[r],
+                           bar);
+    }
+}
+FUGAL_DEVICE bool xwait(uint64_t* xbar, int xi, int* err, unsigned hint_ns) {
+    return mbar_wait(&xbar[xi % kXSlots], static_cast<uint32_t>((xi / kXSlots) & 1), err, hint_ns);
 }
 
 // Reductions over the C x WARPS partials of one row held in slot `slot`: every
@@ -348,12 +373,27 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     }
     if (tid == 0) {
         for (int s = 0; s < p.stages; ++s) mbar_init(&full[s], 1);
-        mbar_init(&xbar[0], 1);
-        mbar_init(&xbar[1], 1);
+        for (int s = 0; s < kXSlots; ++s) mbar_init(&xbar[s], 1);
         fence_mbarrier_init();
         abort_s = 0;
     }
+    // Pipelined 16-bit fast sweeps: the exponentials of a batch wait in tensor
+    // memory (TMEM) for their row normaliser while the next batch is computed.
+    // Warp w uses TMEM lanes 32 (w % 4) .. +31; the warps that share a lane
+    // quarter take separate 64-column halves (two 32-column buffers each).
+    constexpr bool PIPE = !ABSORB && sizeof(T) == 2;
+    constexpr uint32_t TCOLS = ((THREADS / 32 + 3) / 4) * 64;
+    __shared__ uint32_t tmem_slot;
+    const bool pipelined = PIPE && p.pipeline != 0 && !exact_only;  // uniform
+    if constexpr (PIPE) {
+        if (pipelined && (tid >> 5) == 0) {
+            tmem_alloc(&tmem_slot, TCOLS);
+            tmem_relinquish();
+        }
+        tmem_fence_before_sync();
+    }
     __syncthreads();
+    if constexpr (PIPE) tmem_fence_after_sync();
     cluster_sync();  // every peer's barriers exist before the first remote transaction
 
     auto issue = [&](int bt) {
@@ -407,6 +447,230 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     int xuse = 0;
     bool alive = true;
     int bt = 0;
+    if (pipelined) {
+        if constexpr (PIPE) {
+            const int warp = tid >> 5;
+            const uint32_t tcol = tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) +
+                                  static_cast<uint32_t>((warp >> 2) * 64);
+            int x_prev = -1;   // exchange of the batch whose column sums are pending
+            float S_early[R];  // that batch's row sums when they were read ahead (fallback)
+            bool early = false;
+            int waited = 0;    // batches whose stage wait completed
+            for (int it = 0; it <= nbatch; ++it) {
+                int x_cur = -1;
+                if (it < nbatch) {
+                    // ---- batch it.  The 16-bit copy is absorbed (each row's normaliser was
+                    // ~0 when it was written), so 2^(L log2e + b) stays in range without the
+                    // previous row normaliser as reference; a row whose sum leaves the range
+                    // goes to the max-stabilised fallback below.
+                    const int s = it % p.stages;
+                    if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((it / p.stages) & 1), &st->status,
+                                         p.suspend_ns))) {
+                        alive = false;
+                        break;
+                    }
+                    waited = it + 1;
+                    const int rows = min(R, row_end - (row_begin + it * R));
+                    const T* stage = reinterpret_cast<const T*>(stage_base + s * stage_bytes);
+                    float2 e[R][H];
+                    float2 s2[R], t2[R];
+                    float sm[R], zero[R];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        s2[r] = make_float2(0.f, 0.f);
+                        t2[r] = make_float2(0.f, 0.f);
+                        zero[r] = 0.f;
+                    }
+#pragma unroll
+                    for (int g = 0; g < G; ++g) {
+                        const int c = (g * THREADS + tid) * V;
+                        float2 b2[VP];
+                        load_b2(c, b2);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            if (r < rows) {
+                                float2 v2[VP];
+                                Pairs<T>::unpack(
+                                    *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c), v2);
+#pragma unroll
+                                for (int q = 0; q < VP; ++q) {
+                                    const float2 y = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[q]));
+                                    e[r][g * VP + q] = y;
+                                    if (q & 1)
+                                        t2[r] = __fadd2_rn(t2[r], y);
+                                    else
+                                        s2[r] = __fadd2_rn(s2[r], y);
+                                }
+                            } else {
+#pragma unroll
+                                for (int q = 0; q < VP; ++q) e[r][g * VP + q] = make_float2(0.f, 0.f);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const float2 u2 = __fadd2_rn(s2[r], t2[r]);
+                        sm[r] = warp_sum(u2.x + u2.y);
+                    }
+                    tmem_st32(tcol + static_cast<uint32_t>((it & 1) * 32), reinterpret_cast<const float*>(&e[0][0]));
+                    x_cur = xuse++;
+                    xsend<THREADS, R>(xch, xbar, C, rank, x_cur, zero, sm);
+                }
+                if (it > 0) {
+                    // ---- batch it - 1: row normaliser, then its column sums from TMEM
+                    const int pb = it - 1;
+                    const int r0 = row_begin + pb * R;
+                    const int rows = min(R, row_end - r0);
+                    float S[R], anew[R], wr[R];
+                    if (early) {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) S[r] = S_early[r];
+                        early = false;
+                    } else {
+                        if (!agree(xwait(xbar, x_prev, &st->status, p.suspend_ns))) {
+                            alive = false;
+                            break;
+                        }
+#pragma unroll
+                        for (int r = 0; r < R; ++r) S[r] = slot_sum<THREADS, R>(xch, x_prev % kXSlots, C, r);
+                    }
+                    bool fast_ok = true;
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (r < rows && !(S[r] > 1e-30f && S[r] < 1e30f)) fast_ok = false;  // uniform
+                    if (fast_ok) {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            anew[r] = -__log2f(S[r]) * kLn2;
+                            wr[r] = __frcp_rn(S[r]);
+                        }
+                        release(pb);  // every warp of the CTA has sent batch pb's partials
+                        float2 y[R][H];
+                        tmem_wait_st();
+                        tmem_ld32(tcol + static_cast<uint32_t>((pb & 1) * 32), reinterpret_cast<float*>(&y[0][0]));
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            if (r < rows) {
+                                const float2 w2 = make_float2(wr[r], wr[r]);
+#pragma unroll
+                                for (int h = 0; h < H; ++h) acc[h] = __ffma2_rn(y[r][h], w2, acc[h]);
+                            }
+                        }
+                    } else {
+                        // Some row left the fast path's range: read the exchange in flight
+                        // ahead, then redo batch pb (still staged) with the max-stabilised
+                        // reduction: maximum exchange, sum exchange, column sums.
+                        if (x_cur >= 0) {
+                            if (!agree(xwait(xbar, x_cur, &st->status, p.suspend_ns))) {
+                                alive = false;
+                                break;
+                            }
+#pragma unroll
+                            for (int r = 0; r < R; ++r) S_early[r] = slot_sum<THREADS, R>(xch, x_cur % kXSlots, C, r);
+                            early = true;
+                        }
+                        const T* stage = reinterpret_cast<const T*>(stage_base + (pb % p.stages) * stage_bytes);
+                        float mx[R], zero[R], sm[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            mx[r] = -INFINITY;
+                            zero[r] = 0.f;
+                        }
+#pragma unroll
+                        for (int g = 0; g < G; ++g) {
+                            const int c = (g * THREADS + tid) * V;
+                            float2 b2[VP];
+                            load_b2(c, b2);
+#pragma unroll
+                            for (int r = 0; r < R; ++r) {
+                                if (r < rows) {
+                                    float2 v2[VP];
+                                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(
+                                                         stage + static_cast<size_t>(r) * p.slice_w + c),
+                                                     v2);
+#pragma unroll
+                                    for (int q = 0; q < VP; ++q) {
+                                        const float2 x = __ffma2_rn(v2[q], log2e2, b2[q]);
+                                        mx[r] = fmaxf(mx[r], fmaxf(x.x, x.y));
+                                    }
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < R; ++r) mx[r] = warp_max(mx[r]);
+                        int xi = xuse++;
+                        xsend<THREADS, R>(xch, xbar, C, rank, xi, mx, zero);
+                        if (!agree(xwait(xbar, xi, &st->status, p.suspend_ns))) {
+                            alive = false;
+                            break;
+                        }
+                        float M2[R];
+                        float2 e[R][H];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            M2[r] = slot_max<THREADS, R>(xch, xi % kXSlots, C, r);
+                            sm[r] = 0.f;
+                        }
+#pragma unroll
+                        for (int g = 0; g < G; ++g) {
+                            const int c = (g * THREADS + tid) * V;
+                            float2 b2[VP];
+                            load_b2(c, b2);
+#pragma unroll
+                            for (int r = 0; r < R; ++r) {
+                                const float base = (M2[r] == -INFINITY) ? 0.f : M2[r];
+                                const float2 nb = make_float2(-base, -base);
+                                if (r < rows) {
+                                    float2 v2[VP];
+                                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(
+                                                         stage + static_cast<size_t>(r) * p.slice_w + c),
+                                                     v2);
+#pragma unroll
+                                    for (int q = 0; q < VP; ++q) {
+                                        const float2 y = ex2_pair(__fadd2_rn(__ffma2_rn(v2[q], log2e2, b2[q]), nb));
+                                        e[r][g * VP + q] = y;
+                                        sm[r] += y.x + y.y;
+                                    }
+                                } else {
+#pragma unroll
+                                    for (int q = 0; q < VP; ++q) e[r][g * VP + q] = make_float2(0.f, 0.f);
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < R; ++r) sm[r] = warp_sum(sm[r]);
+                        xi = xuse++;
+                        xsend<THREADS, R>(xch, xbar, C, rank, xi, zero, sm);
+                        if (!agree(xwait(xbar, xi, &st->status, p.suspend_ns))) {
+                            alive = false;
+                            break;
+                        }
+                        release(pb);  // every warp has finished reading batch pb's stage
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            const float Sr = slot_sum<THREADS, R>(xch, xi % kXSlots, C, r);
+                            anew[r] = -(M2[r] + log2f(Sr)) * kLn2;
+                            wr[r] = (M2[r] == -INFINITY) ? 0.f : ex2(M2[r] + anew[r] * kLog2e);
+                            if (r < rows) {
+                                const float2 w2 = make_float2(wr[r], wr[r]);
+#pragma unroll
+                                for (int h = 0; h < H; ++h) acc[h] = __ffma2_rn(e[r][h], w2, acc[h]);
+                            }
+                        }
+                    }
+                    if (rank == 0 && tid < rows) {
+                        float v = anew[0];
+#pragma unroll
+                        for (int r = 1; r < R; ++r)
+                            if (tid == r) v = anew[r];
+                        p.a[r0 + tid] = v;
+                    }
+                }
+                x_prev = x_cur;
+            }
+            bt = waited;
+        }
+    } else
     for (; bt < nbatch; ++bt) {
         const int s = bt % p.stages;
         if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status, p.suspend_ns))) {
@@ -625,6 +889,14 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     if (!alive && tid == 0) {
         for (int b = bt; b < issued; ++b)
             if (!mbar_wait(&full[b % p.stages], static_cast<uint32_t>((b / p.stages) & 1), &st->status)) break;
+    }
+    // Tensor memory goes back once every warp's TMEM accesses have completed.
+    if constexpr (PIPE) {
+        if (pipelined) tmem_wait_st();
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        if (pipelined && (tid >> 5) == 0) tmem_dealloc(tmem_slot, TCOLS);
     }
     // No CTA leaves while a peer may still send into its shared memory; the
     // non-aligned form tolerates threads that left the batch loop early.
@@ -887,6 +1159,12 @@ unsigned suspend_hint() {
     return static_cast<unsigned>(v < 0 ? 0 : (v > 1000000 ? 1000000 : v));
 }
 
+// TMEM-pipelined 16-bit fast sweeps (FUGAL_SWEEP_PIPELINE=1 turns them on).
+int pipeline_choice() {
+    const char* e = getenv("FUGAL_SWEEP_PIPELINE");
+    return (e != nullptr && atoi(e) != 0) ? 1 : 0;
+}
+
 // Launch shapes: (threads per CTA, columns per thread).  Rows per batch are
 // 32 / columns-per-thread, so a thread always holds 32 exponentials.
 constexpr int rows_per_batch(int kpt) { return 32 / kpt; }
@@ -961,9 +1239,10 @@ fugal_status plan_shape(int64_t n, int& threads, int& kpt, int& cluster) {
     return FUGAL_OK;
 }
 
-// Dynamic shared memory per CTA kept near 100 KB so two CTAs (of up to 256
-// threads) share an SM and hide each other's exchange latency.
-constexpr int kSmemTarget = 100 * 1024;
+// Dynamic shared memory per CTA kept near 110 KB (with the whole L1 carved out as
+// shared memory) so two CTAs (of up to 256 threads) share an SM and hide each
+// other's exchange latency.
+constexpr int kSmemTarget = 110 * 1024;
 
 fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_occupancy) {
     FUGAL_TRY(plan_shape(n, pl.threads, pl.kpt, pl.cluster));
@@ -992,6 +1271,10 @@ fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_oc
         if (query_occupancy) {
             FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem),
                                  "sinkhorn: set dynamic shared memory"));
+            // all of the unified L1 / shared memory as shared memory, so two CTAs fit per SM
+            FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                      cudaSharedmemCarveoutMaxShared),
+                                 "sinkhorn: shared memory carveout"));
             if (pl.cluster > 8)
                 FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
                                      "sinkhorn: allow cluster size 16"));
@@ -1205,6 +1488,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         a.rows_per_cluster = pl.rows_per_cluster;
         a.rows_pad = pl.rows_pad;
         a.suspend_ns = suspend_hint();
+        a.pipeline = pipeline_choice();
         a.stages = pl.stages;
         a.b_buf = w.b_buf;
         a.b_buf_w = w.b_buf;
