@@ -72,6 +72,8 @@ SIGNATURES = {
     "fugal_exact_lap_workspace_size": (_INT, [_I64, POINTER(c_size_t)]),
     "fugal_exact_lap": (_INT, [_P, _I64, _I64, _INT, _I64, _P, _P, _P, _P, _SZ, _P]),
     "fugal_count_le": (_INT, [_P, _I64, _I64, _F, _P, _P]),
+    "fugal_alignment_overlap_workspace_size": (_INT, [_I64, POINTER(c_size_t)]),
+    "fugal_alignment_overlap": (_INT, [_P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _SZ, _P]),
     "fugal_gradient_workspace_size": (_INT, [_I64, POINTER(c_size_t)]),
     "fugal_fw_gradient": (_INT, [_I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _I64, _D, _D, _D, _P, _P, _P, _I64,
                                  _P, _SZ, _P]),

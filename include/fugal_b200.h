@@ -164,6 +164,21 @@ fugal_status fugal_exact_lap(const float* P, int64_t ldp, int64_t n, int maximiz
 fugal_status fugal_count_le(const float* P, int64_t ldp, int64_t n, float threshold, int64_t* count,
                             fugal_stream_t stream);
 
+/* Overlap of an alignment with the planted one, the integer behind the
+ * reference's EC / ICS / S3 metrics (benchmark/experiment.py:115-144):
+ *   *overlap = |{(i, j) : A[answer_i][answer_j] = 1 and B[truth_i][truth_j] = 1}|
+ * over the stored entries of the CSR graphs A and B (columns sorted per row).
+ * answer and truth are int64 device arrays of length n.  *not_permutation
+ * (device int32) gets bit 0 when answer is not a permutation of 0..n-1 (overlap
+ * not computed; use the dense definition) and bit 1 when truth has an entry
+ * outside 0..n-1. */
+fugal_status fugal_alignment_overlap_workspace_size(int64_t n, size_t* bytes);
+fugal_status fugal_alignment_overlap(const int32_t* a_row_pointers, const int32_t* a_col_indices,
+                                     const int32_t* b_row_pointers, const int32_t* b_col_indices, int64_t n,
+                                     const int64_t* answer, const int64_t* truth, uint64_t* overlap,
+                                     int32_t* not_permutation, void* workspace, size_t workspace_bytes,
+                                     fugal_stream_t stream);
+
 /* ======================= fused Frank-Wolfe step (cugal/pred.py:89-148) ===== */
 
 /* Gradient with the Sinkhorn kernel matrix fused into its epilogue

@@ -524,3 +524,31 @@ def cugal(source, target, p: OracleParams, features: str = "cuda", trace: FWTrac
     cols = hungarian(P, p.hungarian_method, **lap_kw)
     mapping = [(i, int(cols[i])) for i in range(len(P))]
     return P, mapping, sp
+
+
+# ----------------------------------------------------------------- metrics
+def alignment_overlap(A: np.ndarray, B: np.ndarray, answer, truth) -> tuple[int, int, int]:
+    """(overlap, entries of A, entries of the permuted B) behind the metrics of
+    ``benchmark/experiment.py:115-141``: adj1 = A[answer][:, answer],
+    adj2 = B[truth][:, truth], overlap = #(adj1 + adj2 == 2)."""
+    adj1 = A[np.asarray(answer)][:, np.asarray(answer)]
+    adj2 = B[np.asarray(truth)][:, np.asarray(truth)]
+    return int(np.sum(adj1 + adj2 == 2)), int(np.sum(A == 1)), int(np.sum(adj2 == 1))
+
+
+def edge_correctness(A, B, answer, truth) -> float:
+    """``benchmark/experiment.py:115-121``."""
+    inter, na, _ = alignment_overlap(A, B, answer, truth)
+    return inter / na
+
+
+def induced_conserved_structure(A, B, answer, truth) -> float:
+    """``benchmark/experiment.py:124-130``."""
+    inter, _, nb = alignment_overlap(A, B, answer, truth)
+    return inter / nb
+
+
+def symmetric_substructure(A, B, answer, truth) -> float:
+    """``benchmark/experiment.py:133-140``."""
+    inter, na, nb = alignment_overlap(A, B, answer, truth)
+    return inter / (na + nb - inter)
