@@ -37,6 +37,25 @@ FUGAL_DEVICE void report_error(int* flag, int code) {
     if (flag != nullptr) atomicCAS(flag, 0, code);
 }
 
+// SinkhornState.lehmann_momentum (cugal/sinkhorn.py:78-88) over the recorded
+// errors, with Python list indexing (negative indices count from the end).
+FUGAL_DEVICE double lehmann_omega(const double* errors, int len, int eval_freq, int momentum_start) {
+    if (momentum_start < 0 || (long long)len * eval_freq < momentum_start) return 1.0;
+    const int index = momentum_start / eval_freq;
+    if (len < index - 1) return 1.0;
+    int i1 = index - 1, i2 = index - 2;
+    if (i1 < 0) i1 += len;
+    if (i2 < 0) i2 += len;
+    if (i1 < 0 || i2 < 0 || i1 >= len || i2 >= len || i1 >= FUGAL_MAX_RECORDED_ERRORS ||
+        i2 >= FUGAL_MAX_RECORDED_ERRORS)
+        return 1.0;
+    double ratio = errors[i1] / errors[i2];
+    if (isnan(ratio)) ratio = 0.99;
+    ratio = fmin(ratio, 0.99);
+    const double power = 1.0 / eval_freq;
+    return 2.0 / (1.0 + sqrt(1.0 - pow(ratio, power)));
+}
+
 // ---------------------------------------------------------------- reductions
 FUGAL_DEVICE float warp_max(float v) {
 #pragma unroll

@@ -81,24 +81,8 @@ struct SolveState {
 
 // ------------------------------------------------------------------ device
 
-// SinkhornState.lehmann_momentum (cugal/sinkhorn.py:78-88) with Python list
-// indexing (negative indices count from the end).
 __device__ double lehmann_momentum(const SolveState* st) {
-    const int len = st->n_err;
-    if (st->momentum_start < 0 || (long long)len * st->eval_freq < st->momentum_start) return 1.0;
-    const int index = st->momentum_start / st->eval_freq;
-    if (len < index - 1) return 1.0;
-    int i1 = index - 1, i2 = index - 2;
-    if (i1 < 0) i1 += len;
-    if (i2 < 0) i2 += len;
-    if (i1 < 0 || i2 < 0 || i1 >= len || i2 >= len || i1 >= FUGAL_MAX_RECORDED_ERRORS ||
-        i2 >= FUGAL_MAX_RECORDED_ERRORS)
-        return 1.0;
-    double ratio = st->errors[i1] / st->errors[i2];
-    if (isnan(ratio)) ratio = 0.99;
-    ratio = fmin(ratio, 0.99);
-    const double power = 1.0 / st->eval_freq;
-    return 2.0 / (1.0 + sqrt(1.0 - pow(ratio, power)));
+    return lehmann_omega(st->errors, st->n_err, st->eval_freq, st->momentum_start);
 }
 
 // End-of-sweep decision (single thread).

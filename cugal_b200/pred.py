@@ -33,14 +33,17 @@ from .feature_extraction import Features
 from .exact_lap import FUGAL_ITER_LIMIT, FUGAL_OK, exact_assign
 from .greedy_lap import greedy_assign
 from .profile import Phase, Profile, SinkhornProfile, TimeStamp
-from .sinkhorn import SinkhornSolver, padded_ld, read_record
+from .sinkhorn import SinkhornSolver, StandardSolver, exp_scale, padded_ld, read_record
 
 
 def check_config(config: Config) -> None:
     if "cuda" not in str(config.device):
         raise ValueError("cugal_b200 runs on CUDA devices only (config.device must be 'cuda[:k]')")
-    if config.sinkhorn_method != SinkhornMethod.LOG:
-        raise NotImplementedError(f"sinkhorn_method={config.sinkhorn_method.value} is not available; use LOG")
+    if config.sinkhorn_method not in (SinkhornMethod.LOG, SinkhornMethod.STANDARD):
+        raise NotImplementedError(f"sinkhorn_method={config.sinkhorn_method.value} is not available; "
+                                  "use LOG or STANDARD")
+    if config.sinkhorn_method == SinkhornMethod.STANDARD and config.stream_dtype is not None:
+        raise NotImplementedError("stream_dtype (reduced-precision streaming) needs sinkhorn_method=LOG")
     if config.dtype != torch.float32:
         raise NotImplementedError("config.dtype must be torch.float32 on the GPU path "
                                   "(set stream_dtype for BF16/FP16 streaming)")
@@ -78,7 +81,15 @@ class FrankWolfeEngine:
         self.gap = torch.zeros(1, dtype=torch.float64, device=dev)
         self.grad_ws = torch.empty(N.workspace_size("fugal_gradient_workspace_size", n), dtype=torch.uint8,
                                    device=dev)
-        self.solver = SinkhornSolver(n, self.config, dev)
+        self.standard = self.config.sinkhorn_method == SinkhornMethod.STANDARD
+        if self.standard:
+            # scaling form: plain gradient C in cost32, K = exp(-C/reg), scaling vectors from 1/n
+            self.K_buf = torch.zeros((n, self.ld), dtype=torch.float32, device=dev)
+            self.u.fill_(1.0 / n)
+            self.v.fill_(1.0 / n)
+            self.solver = StandardSolver(n, self.config, dev)
+        else:
+            self.solver = SinkhornSolver(n, self.config, dev)
         self.records = torch.empty((max(1, self.max_solves), N.RECORD_BYTES), dtype=torch.uint8, device=dev)
         self.solves = 0
         if isinstance(self.features, Features):
@@ -98,6 +109,10 @@ class FrankWolfeEngine:
     def gradient(self, lam: float, out_scale: float | None = None, out: torch.Tensor | None = None,
                  absorbed: bool = True) -> torch.Tensor:
         reg = self.config.sinkhorn_regularization
+        if self.standard and out is None and out_scale is None:
+            C = self.gradient(lam, out_scale=1.0, out=self.cost32, absorbed=False)
+            exp_scale(C, -1.0 / reg, self.K_buf)
+            return C
         out = self.cost32 if out is None else out
         scale = (-1.0 / reg) if out_scale is None else out_scale
         N.call("fugal_fw_gradient", self.n, self.A.row_pointers.data_ptr(), self.A.col_indices.data_ptr(),
@@ -112,11 +127,19 @@ class FrankWolfeEngine:
         k = self.solves
         if k >= self.records.shape[0]:
             self.records = torch.cat([self.records, torch.empty_like(self.records)])
-        self.solver.solve(self.cost32, self.u, self.v, self.records[k].data_ptr())
+        if self.standard:
+            self.solver.solve(self.K_buf, self.u, self.v, self.records[k].data_ptr())
+        else:
+            self.solver.solve(self.cost32, self.u, self.v, self.records[k].data_ptr())
         self.solves += 1
         return k
 
     def update(self, alpha: float) -> torch.Tensor:
+        if self.standard:
+            N.call("fugal_fw_update_standard", self.n, self.P_buf.data_ptr(), self.ld, self.K_buf.data_ptr(), self.ld,
+                   self.u.data_ptr(), self.v.data_ptr(), self.cost32.data_ptr(), self.ld, float(alpha),
+                   self.gap.data_ptr(), N.stream_handle(self.device))
+            return self.gap
         N.call("fugal_fw_update", self.n, self.P_buf.data_ptr(), self.ld, self.cost32.data_ptr(), self.ld,
                self.u.data_ptr(), self.v.data_ptr(), self.U.data_ptr(), self.V.data_ptr(), float(alpha),
                float(self.config.sinkhorn_regularization), self.gap.data_ptr(), 1, N.stream_handle(self.device))

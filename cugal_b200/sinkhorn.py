@@ -87,17 +87,56 @@ def read_record(raw: torch.Tensor) -> SinkhornProfile:
     return SinkhornProfile(errors=errors, iteration_count=rec.iteration_count, final_error=final)
 
 
+class StandardSolver:
+    """Workspace of the scaling-form solve (``fugal_sinkhorn_standard_solve``) for size n."""
+
+    def __init__(self, n: int, config: Config, device):
+        self.n = n
+        self.config = config
+        self.device = torch.device(device)
+        ws = N.workspace_size("fugal_sinkhorn_standard_workspace_size", n)
+        self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
+
+    def solve(self, K: torch.Tensor, u: torch.Tensor, v: torch.Tensor, record_ptr: int | None = None):
+        """Updates the FP32 scaling vectors u, v in place on the kernel matrix K."""
+        N.require_cuda(K, "K", torch.float32)
+        c = self.config
+        N.call("fugal_sinkhorn_standard_solve", K.data_ptr(), N.matrix_ld(K, "K"), self.n, u.data_ptr(),
+               v.data_ptr(), c.sinkhorn_iterations, c.sinkhorn_threshold, c.sinkhorn_eval_freq,
+               -1 if c.sinkhorn_momentum_start is None else int(c.sinkhorn_momentum_start), record_ptr,
+               self.workspace.data_ptr(), self.workspace.numel(), N.stream_handle(self.device))
+
+
+def exp_scale(C: torch.Tensor, scale: float, out: torch.Tensor) -> torch.Tensor:
+    """out = exp(scale * C) for square row-major FP32 device matrices."""
+    n = C.shape[0]
+    N.call("fugal_exp_scale", C.data_ptr(), N.matrix_ld(C, "C"), n, float(scale), out.data_ptr(),
+           N.matrix_ld(out, "out"), N.stream_handle(C.device))
+    return out
+
+
 class SinkhornState:
-    """Warm-started dual potentials (reference ``cugal/sinkhorn.py:51-65``)."""
+    """Warm-started dual potentials (reference ``cugal/sinkhorn.py:51-65``).
+
+    LOG: log-domain duals (FP64 internally, see the module docstring).  STANDARD:
+    the scaling vectors u, v (FP32, start at 1/n) of ``solve_standard``."""
 
     def __init__(self, n: int, config: Config):
-        if config.sinkhorn_method != SinkhornMethod.LOG:
-            raise NotImplementedError(f"{config.sinkhorn_method} is not available on the GPU path; use LOG")
+        if config.sinkhorn_method not in (SinkhornMethod.LOG, SinkhornMethod.STANDARD):
+            raise NotImplementedError(f"{config.sinkhorn_method} is not available on the GPU path")
         if "cuda" not in config.device:
             raise ValueError("SinkhornState: only CUDA devices are supported")
         self.n = n
         self.config = config
         dev = torch.device(config.device)
+        if config.sinkhorn_method == SinkhornMethod.STANDARD:
+            self.method = SinkhornMethod.STANDARD
+            self.u_std = torch.full((n,), 1.0 / n, dtype=torch.float32, device=dev)
+            self.v_std = torch.full((n,), 1.0 / n, dtype=torch.float32, device=dev)
+            self._std = StandardSolver(n, config, dev)
+            self._rec = torch.empty(N.RECORD_BYTES, dtype=torch.uint8, device=dev)
+            return
+        self.method = SinkhornMethod.LOG
         self.U = torch.zeros(n, dtype=torch.float64, device=dev)
         self.V = torch.zeros(n, dtype=torch.float64, device=dev)
         self._solver = SinkhornSolver(n, config, dev)
@@ -107,15 +146,36 @@ class SinkhornState:
 
     @property
     def u(self) -> torch.Tensor:
+        if self.method == SinkhornMethod.STANDARD:
+            return self.u_std
         return self.U.to(self.config.dtype)
 
     @property
     def v(self) -> torch.Tensor:
+        if self.method == SinkhornMethod.STANDARD:
+            return self.v_std
         return self.V.to(self.config.dtype)
+
+    def solve_standard(self, C: torch.Tensor, config: Config | None = None, profile: SinkhornProfile | None = None):
+        """``solve_standard`` (``cugal/sinkhorn.py:122-144``): returns (K, u, v), K = exp(-C/reg)."""
+        config = config or self.config
+        start = TimeStamp(config.device)
+        N.require_cuda(C, "C")
+        C32 = C.to(torch.float32).contiguous()
+        K = exp_scale(C32, -1.0 / config.sinkhorn_regularization, torch.empty_like(C32))
+        self._std.solve(K, self.u_std, self.v_std, self._rec.data_ptr())
+        if profile is not None:
+            rec = read_record(self._rec.cpu())
+            profile.errors, profile.iteration_count = rec.errors, rec.iteration_count
+            profile.final_error = rec.final_error
+            profile.time = TimeStamp(config.device).elapsed_seconds(start)
+        return K, self.u_std, self.v_std
 
     def solve(self, C: torch.Tensor, config: Config | None = None, profile: SinkhornProfile | None = None):
         """``solve`` / ``solve_log`` (``cugal/sinkhorn.py:90-120,146-156``): returns (K, u, v)."""
         config = config or self.config
+        if self.method == SinkhornMethod.STANDARD:
+            return self.solve_standard(C, config, profile)
         start = TimeStamp(config.device)
         n = self.n
         N.require_cuda(C, "C")

@@ -179,6 +179,27 @@ fugal_status fugal_alignment_overlap(const int32_t* a_row_pointers, const int32_
                                      int32_t* not_permutation, void* workspace, size_t workspace_bytes,
                                      fugal_stream_t stream);
 
+/* Scaling-form Sinkhorn, SinkhornState.solve_standard (cugal/sinkhorn.py:122-144),
+ * on K = exp(-C/reg) (FP32, n x n, ldk): per iteration
+ *   v <- v^(1-w) (1 / (u K + 1e-16))^w,  u <- u^(1-w) (1 / (K v + 1e-16))^w,
+ * the column-marginal error sum_j |sum_i u_i K_ij v_j - 1| at iterations 0,
+ * eval_freq, 2 eval_freq, ... (stop below threshold, Lehmann momentum from
+ * momentum_start, < 0 for none), at most max_iterations iterations.  u, v (FP32,
+ * device) are read and written in place (warm start).  record: optional DEVICE
+ * fugal_solve_record.  fugal_exp_scale writes out = exp(scale * C) (K from C with
+ * scale = -1/reg); fugal_fw_update_standard is the update of cugal/pred.py:77-86
+ * for this method: q = K v u, P += alpha (q - P), *gap = sum C (q - P) in FP64. */
+fugal_status fugal_sinkhorn_standard_workspace_size(int64_t n, size_t* bytes);
+fugal_status fugal_sinkhorn_standard_solve(const float* K, int64_t ldk, int64_t n, float* u, float* v,
+                                           int max_iterations, double threshold, int eval_freq, int momentum_start,
+                                           void* record, void* workspace, size_t workspace_bytes,
+                                           fugal_stream_t stream);
+fugal_status fugal_exp_scale(const float* C, int64_t ldc, int64_t n, double scale, float* out, int64_t ldo,
+                             fugal_stream_t stream);
+fugal_status fugal_fw_update_standard(int64_t n, float* P, int64_t ldp, const float* K, int64_t ldk, const float* u,
+                                      const float* v, const float* C, int64_t ldc, double alpha, double* gap,
+                                      fugal_stream_t stream);
+
 /* ======================= fused Frank-Wolfe step (cugal/pred.py:89-148) ===== */
 
 /* Gradient with the Sinkhorn kernel matrix fused into its epilogue
