@@ -1223,10 +1223,11 @@ fugal_status plan_shape(int64_t n, int& threads, int& kpt, int& cluster) {
     return FUGAL_OK;
 }
 
-// Dynamic shared memory per CTA kept near 110 KB (with the whole L1 carved out as
+// Dynamic shared memory per CTA kept near 100 KB (with the whole L1 carved out as
 // shared memory) so two CTAs (of up to 256 threads) share an SM and hide each
-// other's exchange latency.
-constexpr int kSmemTarget = 110 * 1024;
+// other's exchange latency; at 104 KB and above the cluster occupancy query
+// already settles on one CTA per SM.
+constexpr int kSmemTarget = 100 * 1024;
 
 fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_occupancy) {
     FUGAL_TRY(plan_shape(n, pl.threads, pl.kpt, pl.cluster));
