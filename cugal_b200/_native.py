@@ -83,6 +83,10 @@ SIGNATURES = {
     "fugal_sinkhorn_standard_solve": (_INT, [_P, _I64, _I64, _P, _P, _INT, _D, _INT, _INT, _P, _P, _SZ, _P]),
     "fugal_exp_scale": (_INT, [_P, _I64, _I64, _D, _P, _I64, _P]),
     "fugal_fw_update_standard": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _I64, _D, _P, _P]),
+    "fugal_sinkhorn_plan": (_INT, [_P, _I64, _I64, _P, _P, _P, _I64, _P]),
+    "fugal_plan_matvec_workspace_size": (_INT, [_I64, POINTER(c_size_t)]),
+    "fugal_plan_matvec": (_INT, [_P, _I64, _P, _I64, _I64, _P, _P, _P, _P, _P, _SZ, _P]),
+    "fugal_sinkhorn_adjoint": (_INT, [_P, _I64, _P, _I64, _I64, _P, _P, _D, _P, _I64, _P]),
     "fugal_sinkhorn_workspace_size": (_INT, [_I64, _INT, POINTER(c_size_t)]),
     "fugal_sinkhorn_plan_info": (_INT, [_I64, _INT, _P]),
     "fugal_sinkhorn_solve": (_INT, [POINTER(SolveParams), _P, _SZ, _P]),

@@ -171,6 +171,16 @@ class SinkhornState:
             profile.time = TimeStamp(config.device).elapsed_seconds(start)
         return K, self.u_std, self.v_std
 
+    def plan(self, out: torch.Tensor | None = None) -> torch.Tensor:
+        """The plan P = exp(K + u + v) of the last LOG solve (n x n FP32)."""
+        if self.method != SinkhornMethod.LOG or not hasattr(self, "_cost32"):
+            raise RuntimeError("plan(): run a LOG solve first")
+        n = self.n
+        out = torch.empty((n, n), dtype=torch.float32, device=self._cost32.device) if out is None else out
+        N.call("fugal_sinkhorn_plan", self._cost32.data_ptr(), self._cost32.stride(0), n, self._du.data_ptr(),
+               self._dv.data_ptr(), out.data_ptr(), N.matrix_ld(out, "out"), N.stream_handle(out.device))
+        return out
+
     def solve(self, C: torch.Tensor, config: Config | None = None, profile: SinkhornProfile | None = None):
         """``solve`` / ``solve_log`` (``cugal/sinkhorn.py:90-120,146-156``): returns (K, u, v)."""
         config = config or self.config
@@ -183,6 +193,7 @@ class SinkhornState:
         cost32 = torch.zeros((n, padded_ld(n)), dtype=torch.float32, device=C.device)  # finite padding
         cost32[:, :n] = (K.double() + self.U[:, None] + self.V[None, :]).float()
         self._solver.solve(cost32, self._du, self._dv, self._rec.data_ptr())
+        self._cost32 = cost32
         self.U += self._du.double()
         self.V += self._dv.double()
         if profile is not None:

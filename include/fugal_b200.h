@@ -200,6 +200,23 @@ fugal_status fugal_fw_update_standard(int64_t n, float* P, int64_t ldp, const fl
                                       const float* v, const float* C, int64_t ldc, double alpha, double* gap,
                                       fugal_stream_t stream);
 
+/* Differentiation of the log-domain solve (no counterpart in the reference, which
+ * has no backward pass; the torch autograd of its solve_log is the check).
+ * fugal_sinkhorn_plan: P = exp(cost32 + u_i + v_j).  fugal_plan_matvec: with
+ * M = P (W == NULL) or P o W, Py = M y and Ptx = M^T x (FP64 vectors, one pass
+ * over M).  fugal_sinkhorn_adjoint: out = scale * P o (G - alpha_i - beta_j), the
+ * cost gradient of the implicit adjoint (scale = -1/reg) once alpha, beta solve
+ * [I P; P^T I][alpha; beta] = [(P o G) 1; (P o G)^T 1]. */
+fugal_status fugal_sinkhorn_plan(const float* cost32, int64_t ld32, int64_t n, const float* u, const float* v,
+                                 float* P, int64_t ldp, fugal_stream_t stream);
+fugal_status fugal_plan_matvec_workspace_size(int64_t n, size_t* bytes);
+fugal_status fugal_plan_matvec(const float* P, int64_t ldp, const float* W, int64_t ldw, int64_t n,
+                               const double* x, const double* y, double* Ptx, double* Py, void* workspace,
+                               size_t workspace_bytes, fugal_stream_t stream);
+fugal_status fugal_sinkhorn_adjoint(const float* P, int64_t ldp, const float* G, int64_t ldg, int64_t n,
+                                    const double* alpha, const double* beta, double scale, float* out, int64_t ldo,
+                                    fugal_stream_t stream);
+
 /* ======================= fused Frank-Wolfe step (cugal/pred.py:89-148) ===== */
 
 /* Gradient with the Sinkhorn kernel matrix fused into its epilogue

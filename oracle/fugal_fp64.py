@@ -552,3 +552,24 @@ def symmetric_substructure(A, B, answer, truth) -> float:
     """``benchmark/experiment.py:133-140``."""
     inter, na, nb = alignment_overlap(A, B, answer, truth)
     return inter / (na + nb - inter)
+
+
+# ------------------------------------------------------------ differentiation
+def sinkhorn_plan_log(C: np.ndarray, reg: float, max_iter: int = 5000, threshold: float = 1e-14,
+                      eval_freq: int = 10) -> np.ndarray:
+    """Converged plan P = exp(-C/reg + u + v) of the log-domain solve
+    (``cugal/sinkhorn.py:90-120``) from zero potentials, FP64."""
+    n = C.shape[0]
+    res = sinkhorn_log_solve(C, np.zeros(n), np.zeros(n), reg, max_iter, threshold, eval_freq, None, False)
+    return np.exp(res.K + res.u[:, None] + res.v[None, :])
+
+
+def sinkhorn_implicit_adjoint(P: np.ndarray, G: np.ndarray, reg: float) -> np.ndarray:
+    """dL/dC at a converged plan P for G = dL/dP (implicit differentiation of the
+    unit row / column sums): solve [I P; P^T I][a; b] = [(G o P) 1; (G o P)^T 1]
+    (least squares: one null vector), dL/dC = -(1/reg) P o (G - a 1^T - 1 b^T)."""
+    n = P.shape[0]
+    GP = G * P
+    M = np.block([[np.eye(n), P], [P.T, np.eye(n)]])
+    z = np.linalg.lstsq(M, np.concatenate([GP.sum(1), GP.sum(0)]), rcond=None)[0]
+    return -(P * (G - z[:n, None] - z[None, n:])) / reg
