@@ -87,6 +87,7 @@ SIGNATURES = {
     "fugal_plan_matvec_workspace_size": (_INT, [_I64, POINTER(c_size_t)]),
     "fugal_plan_matvec": (_INT, [_P, _I64, _P, _I64, _I64, _P, _P, _P, _P, _P, _SZ, _P]),
     "fugal_sinkhorn_adjoint": (_INT, [_P, _I64, _P, _I64, _I64, _P, _P, _D, _P, _I64, _P]),
+    "fugal_sinkhorn_unrolled_step_backward": (_INT, [_P, _I64, _I64, _P, _P, _P, _INT, _P, _I64, _P, _P, _SZ, _P]),
     "fugal_sinkhorn_workspace_size": (_INT, [_I64, _INT, POINTER(c_size_t)]),
     "fugal_sinkhorn_plan_info": (_INT, [_I64, _INT, _P]),
     "fugal_sinkhorn_solve": (_INT, [POINTER(SolveParams), _P, _SZ, _P]),

@@ -116,6 +116,92 @@ def sinkhorn_plan(C: torch.Tensor, config: Config, tol: float = 1e-7, max_iter: 
     return SinkhornPlan.apply(C, dataclasses.replace(config, stream_dtype=None), tol, max_iter)
 
 
+class SinkhornPlanUnrolled(torch.autograd.Function):
+    """P after the reference's iteration (cugal/sinkhorn.py:108-115, no momentum)
+    run from zero potentials, differentiated through the iterations: the duals
+    are checkpointed every ``every`` iterations, each segment is recomputed on
+    the way back, and every half step is reversed on the device
+    (``fugal_sinkhorn_unrolled_step_backward``)."""
+
+    @staticmethod
+    def forward(ctx, C, config, every):
+        n = C.shape[0]
+        dev = C.device
+        reg = config.sinkhorn_regularization
+        K = (-C.detach().to(torch.float32) / reg).contiguous()
+        Kt = K.t().contiguous()
+        u = torch.zeros(n, dtype=torch.float32, device=dev)
+        v = torch.zeros(n, dtype=torch.float32, device=dev)
+        stream = N.stream_handle(dev)
+        err = torch.zeros(1, dtype=torch.float64, device=dev)
+        checkpoints = {0: (u.clone(), v.clone())}
+        T = 0
+        for t in range(config.sinkhorn_iterations):
+            N.call("fugal_sinkhorn_log_step", Kt.data_ptr(), n, n, n, u.data_ptr(), v.data_ptr(), 1.0, stream)
+            N.call("fugal_sinkhorn_log_step", K.data_ptr(), n, n, n, v.data_ptr(), u.data_ptr(), 1.0, stream)
+            T = t + 1
+            if T % every == 0:
+                checkpoints[T] = (u.clone(), v.clone())
+            if t % config.sinkhorn_eval_freq == 0 and t != 0:
+                N.call("fugal_sinkhorn_log_marginal", K.data_ptr(), n, n, u.data_ptr(), v.data_ptr(), 0,
+                       err.data_ptr(), stream)
+                if err.item() < config.sinkhorn_threshold:
+                    break
+        P = torch.empty((n, n), dtype=torch.float32, device=dev)
+        N.call("fugal_sinkhorn_plan", K.data_ptr(), n, n, u.data_ptr(), v.data_ptr(), P.data_ptr(), n, stream)
+        ctx.save_for_backward(K, Kt, P)
+        ctx.checkpoints, ctx.T, ctx.every, ctx.reg, ctx.uv = checkpoints, T, every, reg, (u, v)
+        return P
+
+    @staticmethod
+    def backward(ctx, G):
+        K, Kt, P = ctx.saved_tensors
+        n = K.shape[0]
+        dev = K.device
+        stream = N.stream_handle(dev)
+        mv = _Matvec(n, dev)
+        ws = mv.ws
+        ones = torch.ones(n, dtype=torch.float64, device=dev)
+        G = G.to(torch.float32).contiguous()
+        gK = (G * P).contiguous()
+        gv, gu = mv(P, ones, ones, W=G)   # dL/dv_T = (G o P)^T 1, dL/du_T = (G o P) 1
+
+        def step_back(out_dual, other_dual, g, axis, g_other):
+            N.call("fugal_sinkhorn_unrolled_step_backward", K.data_ptr(), n, n, out_dual.data_ptr(),
+                   other_dual.data_ptr(), g.data_ptr(), axis, gK.data_ptr(), n, g_other.data_ptr(), ws.data_ptr(),
+                   ws.numel(), stream)
+
+        T, every = ctx.T, ctx.every
+        seg_end = T
+        while seg_end > 0:
+            seg_start = ((seg_end - 1) // every) * every
+            u, v = (x.clone() for x in ctx.checkpoints[seg_start])
+            states = [(u.clone(), v.clone())]          # (u_t, v_t) for t = seg_start .. seg_end
+            for _ in range(seg_start, seg_end):
+                N.call("fugal_sinkhorn_log_step", Kt.data_ptr(), n, n, n, u.data_ptr(), v.data_ptr(), 1.0, stream)
+                N.call("fugal_sinkhorn_log_step", K.data_ptr(), n, n, n, v.data_ptr(), u.data_ptr(), 1.0, stream)
+                states.append((u.clone(), v.clone()))
+            for t in range(seg_end - 1, seg_start - 1, -1):
+                u_t = states[t - seg_start][0]
+                u_next, v_next = states[t + 1 - seg_start]
+                # row half: u_{t+1} = -LSE_j(K + v_{t+1})
+                step_back(u_next, v_next, gu, 1, gv)
+                # column half: v_{t+1} = -LSE_i(K + u_t)
+                gu = torch.zeros(n, dtype=torch.float64, device=dev)
+                step_back(v_next, u_t, gv, 0, gu)
+                gv = torch.zeros(n, dtype=torch.float64, device=dev)
+            seg_end = seg_start
+        return -gK / ctx.reg, None, None
+
+
+def sinkhorn_plan_unrolled(C: torch.Tensor, config: Config, every: int = 10) -> torch.Tensor:
+    """Differentiable plan of the reference's log-domain iteration, unrolled with
+    dual checkpoints every ``every`` iterations (momentum not supported)."""
+    if config.sinkhorn_method != SinkhornMethod.LOG or config.sinkhorn_momentum_start is not None:
+        raise NotImplementedError("the unrolled adjoint covers SinkhornMethod.LOG without momentum")
+    return SinkhornPlanUnrolled.apply(C.contiguous(), config, every)
+
+
 def adjacency_product(A: Adjacency, M: torch.Tensor) -> torch.Tensor:
     """A @ M for a CSR adjacency and a dense FP32 matrix (device SpMM)."""
     return A.mul(M.contiguous())

@@ -114,6 +114,75 @@ __global__ void adjoint_kernel(const float* __restrict__ P, long long ldp, const
     }
 }
 
+// Backward of one half step of the unrolled log-domain iteration (no momentum).
+// axis 1 (row half, out_i = -LSE_j(K_ij + other_j)):  E_ij = exp(K_ij + other_j + out_i),
+//     gK_ij -= g_i E_ij,   g_other_j -= sum_i g_i E_ij        (column partials)
+// axis 0 (column half, out_j = -LSE_i(K_ij + other_i)): E_ij = exp(K_ij + other_i + out_j),
+//     gK_ij -= g_j E_ij,   g_other_i -= sum_j g_j E_ij        (row partials)
+__global__ void __launch_bounds__(kMvThreads) unrolled_step_kernel(const float* __restrict__ K, long long ldk, int n,
+                                                                   const float* __restrict__ out_dual,
+                                                                   const float* __restrict__ other_dual,
+                                                                   const double* __restrict__ g, int axis,
+                                                                   float* __restrict__ gK, long long ldg,
+                                                                   double* row_part, double* col_part) {
+    __shared__ double red[kMvThreads / 32][kMvRows];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r0 = blockIdx.y * kMvRows;
+    const int j0 = blockIdx.x * kMvCols + threadIdx.x * 4;
+    double cs[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int r = 0; r < kMvRows; ++r) {
+        const int i = r0 + r;
+        double rs = 0.0;
+        if (i < n) {
+            const float* krow = K + static_cast<size_t>(i) * ldk;
+            float* grow = gK + static_cast<size_t>(i) * ldg;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = j0 + q;
+                if (j < n) {
+                    double e, w;
+                    if (axis == 1) {
+                        e = exp(static_cast<double>(krow[j]) + other_dual[j] + out_dual[i]);
+                        w = g[i] * e;
+                        cs[q] -= w;
+                    } else {
+                        e = exp(static_cast<double>(krow[j]) + other_dual[i] + out_dual[j]);
+                        w = g[j] * e;
+                        rs -= w;
+                    }
+                    grow[j] = static_cast<float>(static_cast<double>(grow[j]) - w);
+                }
+            }
+        }
+        if (axis == 0) {
+            rs = warp_sum(rs);
+            if (lane == 0) red[warp][r] = rs;
+        }
+    }
+    if (axis == 0) {
+        __syncthreads();
+        if (threadIdx.x < kMvRows) {
+            const int i = r0 + threadIdx.x;
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < kMvThreads / 32; ++w) s += red[w][threadIdx.x];
+            if (i < n) row_part[static_cast<size_t>(blockIdx.x) * n + i] = s;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (j0 + q < n) col_part[static_cast<size_t>(blockIdx.y) * n + j0 + q] = cs[q];
+    }
+}
+
+__global__ void merge_add_kernel(const double* part, int parts, int n, double* out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int p = 0; p < parts; ++p) s += part[static_cast<size_t>(p) * n + k];
+        out[k] += s;
+    }
+}
+
 inline dim3 ew2d(int64_t n) {
     return dim3(static_cast<unsigned>(std::min<int64_t>((n + 255) / 256, 32)),
                 static_cast<unsigned>(std::min<int64_t>(n, 8 * sm_count())));
@@ -182,4 +251,41 @@ extern "C" fugal_status fugal_sinkhorn_adjoint(const float* P, int64_t ldp, cons
     LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
     adjoint_kernel<<<ew2d(n), 256, 0, stream>>>(P, ldp, G, ldg, static_cast<int>(n), alpha, beta, scale, out, ldo);
     return launch_check("fugal_sinkhorn_adjoint");
+}
+
+extern "C" fugal_status fugal_sinkhorn_unrolled_step_backward(const float* K, int64_t ldk, int64_t n,
+                                                              const float* out_dual, const float* other_dual,
+                                                              const double* g, int axis, float* gK, int64_t ldg,
+                                                              double* g_other, void* workspace,
+                                                              size_t workspace_bytes, fugal_stream_t stream_) {
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    size_t need = 0;
+    FUGAL_TRY(fugal_plan_matvec_workspace_size(n, &need));
+    if (K == nullptr || out_dual == nullptr || other_dual == nullptr || g == nullptr || gK == nullptr ||
+        g_other == nullptr || workspace == nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_unrolled_step_backward: null argument");
+    if (axis != 0 && axis != 1) return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_unrolled_step_backward: axis 0 or 1");
+    if (ldk < n || ldg < n) return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_unrolled_step_backward: bad shape");
+    if (workspace_bytes < need)
+        return fail(FUGAL_WORKSPACE_TOO_SMALL, "fugal_sinkhorn_unrolled_step_backward: workspace too small");
+    const int nn = static_cast<int>(n);
+    const int cb = static_cast<int>((n + kMvCols - 1) / kMvCols), rb = static_cast<int>((n + kMvRows - 1) / kMvRows);
+    double* row_part = static_cast<double*>(workspace);
+    double* col_part = row_part + static_cast<size_t>(cb) * n;
+    {
+        LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
+        unrolled_step_kernel<<<dim3(cb, rb), kMvThreads, 0, stream>>>(K, ldk, nn, out_dual, other_dual, g, axis, gK,
+                                                                      ldg, row_part, col_part);
+        FUGAL_TRY(launch_check("fugal_sinkhorn_unrolled_step_backward"));
+    }
+    {
+        LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
+        const int blocks = static_cast<int>(std::min<int64_t>((n + 255) / 256, 4 * sm_count()));
+        if (axis == 0)
+            merge_add_kernel<<<blocks, 256, 0, stream>>>(row_part, cb, nn, g_other);
+        else
+            merge_add_kernel<<<blocks, 256, 0, stream>>>(col_part, rb, nn, g_other);
+        FUGAL_TRY(launch_check("fugal_sinkhorn_unrolled_step_backward: merge"));
+    }
+    return FUGAL_OK;
 }

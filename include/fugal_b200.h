@@ -216,6 +216,16 @@ fugal_status fugal_plan_matvec(const float* P, int64_t ldp, const float* W, int6
 fugal_status fugal_sinkhorn_adjoint(const float* P, int64_t ldp, const float* G, int64_t ldg, int64_t n,
                                     const double* alpha, const double* beta, double scale, float* out, int64_t ldo,
                                     fugal_stream_t stream);
+/* Unrolled backward of one half step of the log-domain iteration (no momentum),
+ * for the checkpointed unrolled adjoint.  axis 1: out = -LSE_j(K_ij + other_j)
+ * (row update); axis 0: out = -LSE_i(K_ij + other_i) (column update).  With
+ * E = exp(K + other + out) in that orientation and g = dL/d(out) (FP64):
+ * gK -= g o E (FP32, in place) and g_other -= the reduction of g o E over the
+ * LSE axis (FP64, accumulated).  Workspace as fugal_plan_matvec_workspace_size. */
+fugal_status fugal_sinkhorn_unrolled_step_backward(const float* K, int64_t ldk, int64_t n, const float* out_dual,
+                                                   const float* other_dual, const double* g, int axis, float* gK,
+                                                   int64_t ldg, double* g_other, void* workspace,
+                                                   size_t workspace_bytes, fugal_stream_t stream);
 
 /* ======================= fused Frank-Wolfe step (cugal/pred.py:89-148) ===== */
 

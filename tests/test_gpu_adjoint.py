@@ -92,3 +92,15 @@ def test_tune_mu_runs_and_descends():
     assert len(hist) == 5
     assert all(np.isfinite(x) for row in hist for x in row)
     assert hist[-1][0] != hist[0][0]
+
+
+@pytest.mark.parametrize("k,every", [(0, 10), (1, 7)])
+def test_unrolled_adjoint_matches_reference_autograd(k, every):
+    from cugal_b200.autograd import sinkhorn_plan_unrolled
+    C0, W, reg = GOLD[f"C{k}"], GOLD[f"W{k}"], float(GOLD[f"reg{k}"])
+    C = torch.tensor(C0, dtype=torch.float32, device="cuda", requires_grad=True)
+    P = sinkhorn_plan_unrolled(C, _config(reg, iters=300, thr=1e-6), every=every)
+    np.testing.assert_allclose(P.detach().cpu().numpy(), GOLD[f"P{k}"], rtol=1e-3, atol=1e-5)
+    (torch.tensor(W, dtype=torch.float32, device="cuda") * P).sum().backward()
+    ref = GOLD[f"dC{k}"]
+    np.testing.assert_allclose(C.grad.cpu().numpy(), ref, rtol=2e-3, atol=2e-3 * np.abs(ref).max())
