@@ -59,6 +59,8 @@ def parse_args(argv=None):
     ap.add_argument("--sinkhorn-iterations", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune-mu", type=int, default=0, metavar="STEPS",
+                    help="differentiation workload instead: STEPS gradient steps on mu through the Sinkhorn adjoint")
     ap.add_argument("--fp32-warmup-sweeps", type=int, default=None, help="override Config.fp32_warmup_sweeps")
     ap.add_argument("--reabsorb-every", type=int, default=None, help="override Config.reabsorb_every")
     return ap.parse_args(argv)
@@ -404,10 +406,43 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_tune_mu(args):
+    """Differentiation workload (default nws4096): C(mu) = -2 A P0 B + mu D at the
+    uniform P0, the converged FP32 log-Sinkhorn plan P(mu), the structural
+    objective -<P, A P B>, and `--tune-mu` gradient steps on mu from 0.2 through
+    the implicit adjoint; reports seconds per step (forward solve + adjoint)."""
+    from cugal_b200.adjacency import Adjacency
+    from cugal_b200.autograd import tune_mu
+    from cugal_b200.feature_extraction import Features
+    from cugal_b200.synthetic import config_for, make_pair
+    src, tgt, perm, w = make_pair(args.workload, n=args.n)
+    config = config_for(w, device="cuda", mu=1.0, sinkhorn_threshold=1e-4, sinkhorn_iterations=2000)
+    n = src.number_of_nodes()
+    A = Adjacency.from_graph(src, "cuda")
+    B = Adjacency.from_graph(tgt, "cuda")
+    D = Features.create(A, B, config).distance_matrix()[:n, :n].contiguous()
+    P0 = torch.full((n, n), 1.0 / n, device="cuda")
+    tune_mu(A, B, D, config, P0, mu0=0.2, steps=1)  # warm-up
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    hist = tune_mu(A, B, D, config, P0, mu0=0.2, steps=args.tune_mu)
+    stop.record()
+    torch.cuda.synchronize()
+    secs = start.elapsed_time(stop) / 1000.0 / args.tune_mu
+    print(json.dumps({"metric": "mu tuning step (forward solve + implicit adjoint)", "value": secs, "unit": "s/step",
+                      "higher_is_better": False, "n_gpus": 1, "steps": args.tune_mu, "dtype": "f32",
+                      "data": "synthetic", "config": {"workload": w.name, "n": n,
+                                                      "reg": config.sinkhorn_regularization},
+                      "trajectory": [{"mu": m, "objective": o, "dobj_dmu": g} for m, o, g in hist]}), flush=True)
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         run_reference(args)
+    elif args.tune_mu:
+        run_tune_mu(args)
     else:
         run_ours(args)
 
