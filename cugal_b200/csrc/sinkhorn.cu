@@ -125,7 +125,6 @@ struct SweepArgs {
     int rows_per_cluster;
     int rows_pad;         // rows_per_cluster rounded up to 32 (shared staging of the row duals)
     unsigned suspend_ns;  // mbarrier try_wait suspend-time hint of the sweep's waits
-    int pipeline;         // 16-bit fast sweeps: stage exponentials in TMEM, overlap the exchanges
     int stages;
     const float* b_buf;   // [2][n_pad] column duals of consecutive sweeps
     const float* b_off;   // frame offset added to the previous b (nullable)
@@ -176,7 +175,7 @@ FUGAL_DEVICE float lanes_max(float v) {
 //   [128, header)     xch[kXSlots][kMaxCluster][WARPS][R] float2: per-warp row partials of every CTA
 //   [header, +4 W)    b_s[slice_w]: this sweep's column duals for the CTA's slice
 //   then              a_s[rows_pad], stages[stages][R][slice_w] elements of the streamed cost
-constexpr int kXSlots = 4;
+constexpr int kXSlots = 2;
 template <int THREADS, int R>
 __host__ __device__ constexpr int header_bytes_v3() {
     return ((kBarBytes + kXSlots * kMaxCluster * (THREADS / 32) * R * 8) + 127) / 128 * 128;
@@ -205,29 +204,6 @@ __device__ __forceinline__ int exchange(float2* xch, uint64_t* xbar, int C, int 
                            bar);
     }
     return mbar_wait(&xbar[slot], parity, err, hint_ns) ? slot : -1;
-}
-
-// Split form of the exchange for the pipelined sweep: exchange number `xi` uses
-// slot xi % kXSlots.  Every CTA reads the data of exchange j before it sends
-// exchange j + 2 and sends exchange k only after exchange k - 2 has completed,
-// so with four slots a slot is never overwritten while a peer still reads it.
-template <int THREADS, int R>
-__device__ __forceinline__ void xsend(float2* xch, uint64_t* xbar, int C, int rank, int xi, const float* m,
-                                      const float* sm) {
-    constexpr int WARPS = THREADS / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int slot = xi % kXSlots;
-    if (threadIdx.x == 0) mbar_arrive_expect_tx(&xbar[slot], static_cast<uint32_t>(C * WARPS * R * 8));
-    if (lane < C) {
-        const uint32_t bar = map_to_rank(&xbar[slot], lane);
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-            st_async_f32x2(map_to_rank(&xch[((slot * kMaxCluster + rank) * WARPS + warp) * R + r], lane), m[r], sm[r],
-                           bar);
-    }
-}
-FUGAL_DEVICE bool xwait(uint64_t* xbar, int xi, int* err, unsigned hint_ns) {
-    return mbar_wait(&xbar[xi % kXSlots], static_cast<uint32_t>((xi / kXSlots) & 1), err, hint_ns);
 }
 
 // Reductions over the C x WARPS partials of one row held in slot `slot`: every
@@ -361,23 +337,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
         fence_mbarrier_init();
         abort_s = 0;
     }
-    // Pipelined 16-bit fast sweeps: the exponentials of a batch wait in tensor
-    // memory (TMEM) for their row normaliser while the next batch is computed.
-    // Warp w uses TMEM lanes 32 (w % 4) .. +31; the warps that share a lane
-    // quarter take separate 64-column halves (two 32-column buffers each).
-    constexpr bool PIPE = !ABSORB && sizeof(T) == 2;
-    constexpr uint32_t TCOLS = ((THREADS / 32 + 3) / 4) * 64;
-    __shared__ uint32_t tmem_slot;
-    const bool pipelined = PIPE && p.pipeline != 0 && !exact_only;  // uniform
-    if constexpr (PIPE) {
-        if (pipelined && (tid >> 5) == 0) {
-            tmem_alloc(&tmem_slot, TCOLS);
-            tmem_relinquish();
-        }
-        tmem_fence_before_sync();
-    }
     __syncthreads();
-    if constexpr (PIPE) tmem_fence_after_sync();
     cluster_sync();  // every peer's barriers exist before the first remote transaction
 
     auto issue = [&](int bt) {
@@ -431,230 +391,6 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     int xuse = 0;
     bool alive = true;
     int bt = 0;
-    if (pipelined) {
-        if constexpr (PIPE) {
-            const int warp = tid >> 5;
-            const uint32_t tcol = tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) +
-                                  static_cast<uint32_t>((warp >> 2) * 64);
-            int x_prev = -1;   // exchange of the batch whose column sums are pending
-            float S_early[R];  // that batch's row sums when they were read ahead (fallback)
-            bool early = false;
-            int waited = 0;    // batches whose stage wait completed
-            for (int it = 0; it <= nbatch; ++it) {
-                int x_cur = -1;
-                if (it < nbatch) {
-                    // ---- batch it.  The 16-bit copy is absorbed (each row's normaliser was
-                    // ~0 when it was written), so 2^(L log2e + b) stays in range without the
-                    // previous row normaliser as reference; a row whose sum leaves the range
-                    // goes to the max-stabilised fallback below.
-                    const int s = it % p.stages;
-                    if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((it / p.stages) & 1), &st->status,
-                                         p.suspend_ns))) {
-                        alive = false;
-                        break;
-                    }
-                    waited = it + 1;
-                    const int rows = min(R, row_end - (row_begin + it * R));
-                    const T* stage = reinterpret_cast<const T*>(stage_base + s * stage_bytes);
-                    float2 e[R][H];
-                    float2 s2[R], t2[R];
-                    float sm[R], zero[R];
-#pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        s2[r] = make_float2(0.f, 0.f);
-                        t2[r] = make_float2(0.f, 0.f);
-                        zero[r] = 0.f;
-                    }
-#pragma unroll
-                    for (int g = 0; g < G; ++g) {
-                        const int c = (g * THREADS + tid) * V;
-                        float2 b2[VP];
-                        load_b2(c, b2);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            if (r < rows) {
-                                float2 v2[VP];
-                                Pairs<T>::unpack(
-                                    *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c), v2);
-#pragma unroll
-                                for (int q = 0; q < VP; ++q) {
-                                    const float2 y = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[q]));
-                                    e[r][g * VP + q] = y;
-                                    if (q & 1)
-                                        t2[r] = __fadd2_rn(t2[r], y);
-                                    else
-                                        s2[r] = __fadd2_rn(s2[r], y);
-                                }
-                            } else {
-#pragma unroll
-                                for (int q = 0; q < VP; ++q) e[r][g * VP + q] = make_float2(0.f, 0.f);
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const float2 u2 = __fadd2_rn(s2[r], t2[r]);
-                        sm[r] = warp_sum(u2.x + u2.y);
-                    }
-                    tmem_st32(tcol + static_cast<uint32_t>((it & 1) * 32), reinterpret_cast<const float*>(&e[0][0]));
-                    x_cur = xuse++;
-                    xsend<THREADS, R>(xch, xbar, C, rank, x_cur, zero, sm);
-                }
-                if (it > 0) {
-                    // ---- batch it - 1: row normaliser, then its column sums from TMEM
-                    const int pb = it - 1;
-                    const int r0 = row_begin + pb * R;
-                    const int rows = min(R, row_end - r0);
-                    float S[R], anew[R], wr[R];
-                    if (early) {
-#pragma unroll
-                        for (int r = 0; r < R; ++r) S[r] = S_early[r];
-                        early = false;
-                    } else {
-                        if (!agree(xwait(xbar, x_prev, &st->status, p.suspend_ns))) {
-                            alive = false;
-                            break;
-                        }
-#pragma unroll
-                        for (int r = 0; r < R; ++r) S[r] = slot_sum<THREADS, R>(xch, x_prev % kXSlots, C, r);
-                    }
-                    bool fast_ok = true;
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        if (r < rows && !(S[r] > 1e-30f && S[r] < 1e30f)) fast_ok = false;  // uniform
-                    if (fast_ok) {
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            anew[r] = -__log2f(S[r]) * kLn2;
-                            wr[r] = __frcp_rn(S[r]);
-                        }
-                        release(pb);  // every warp of the CTA has sent batch pb's partials
-                        float2 y[R][H];
-                        tmem_wait_st();
-                        tmem_ld32(tcol + static_cast<uint32_t>((pb & 1) * 32), reinterpret_cast<float*>(&y[0][0]));
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            if (r < rows) {
-                                const float2 w2 = make_float2(wr[r], wr[r]);
-#pragma unroll
-                                for (int h = 0; h < H; ++h) acc[h] = __ffma2_rn(y[r][h], w2, acc[h]);
-                            }
-                        }
-                    } else {
-                        // Some row left the fast path's range: read the exchange in flight
-                        // ahead, then redo batch pb (still staged) with the max-stabilised
-                        // reduction: maximum exchange, sum exchange, column sums.
-                        if (x_cur >= 0) {
-                            if (!agree(xwait(xbar, x_cur, &st->status, p.suspend_ns))) {
-                                alive = false;
-                                break;
-                            }
-#pragma unroll
-                            for (int r = 0; r < R; ++r) S_early[r] = slot_sum<THREADS, R>(xch, x_cur % kXSlots, C, r);
-                            early = true;
-                        }
-                        const T* stage = reinterpret_cast<const T*>(stage_base + (pb % p.stages) * stage_bytes);
-                        float mx[R], zero[R], sm[R];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            mx[r] = -INFINITY;
-                            zero[r] = 0.f;
-                        }
-#pragma unroll
-                        for (int g = 0; g < G; ++g) {
-                            const int c = (g * THREADS + tid) * V;
-                            float2 b2[VP];
-                            load_b2(c, b2);
-#pragma unroll
-                            for (int r = 0; r < R; ++r) {
-                                if (r < rows) {
-                                    float2 v2[VP];
-                                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(
-                                                         stage + static_cast<size_t>(r) * p.slice_w + c),
-                                                     v2);
-#pragma unroll
-                                    for (int q = 0; q < VP; ++q) {
-                                        const float2 x = __ffma2_rn(v2[q], log2e2, b2[q]);
-                                        mx[r] = fmaxf(mx[r], fmaxf(x.x, x.y));
-                                    }
-                                }
-                            }
-                        }
-#pragma unroll
-                        for (int r = 0; r < R; ++r) mx[r] = warp_max(mx[r]);
-                        int xi = xuse++;
-                        xsend<THREADS, R>(xch, xbar, C, rank, xi, mx, zero);
-                        if (!agree(xwait(xbar, xi, &st->status, p.suspend_ns))) {
-                            alive = false;
-                            break;
-                        }
-                        float M2[R];
-                        float2 e[R][H];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            M2[r] = slot_max<THREADS, R>(xch, xi % kXSlots, C, r);
-                            sm[r] = 0.f;
-                        }
-#pragma unroll
-                        for (int g = 0; g < G; ++g) {
-                            const int c = (g * THREADS + tid) * V;
-                            float2 b2[VP];
-                            load_b2(c, b2);
-#pragma unroll
-                            for (int r = 0; r < R; ++r) {
-                                const float base = (M2[r] == -INFINITY) ? 0.f : M2[r];
-                                const float2 nb = make_float2(-base, -base);
-                                if (r < rows) {
-                                    float2 v2[VP];
-                                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(
-                                                         stage + static_cast<size_t>(r) * p.slice_w + c),
-                                                     v2);
-#pragma unroll
-                                    for (int q = 0; q < VP; ++q) {
-                                        const float2 y = ex2_pair(__fadd2_rn(__ffma2_rn(v2[q], log2e2, b2[q]), nb));
-                                        e[r][g * VP + q] = y;
-                                        sm[r] += y.x + y.y;
-                                    }
-                                } else {
-#pragma unroll
-                                    for (int q = 0; q < VP; ++q) e[r][g * VP + q] = make_float2(0.f, 0.f);
-                                }
-                            }
-                        }
-#pragma unroll
-                        for (int r = 0; r < R; ++r) sm[r] = warp_sum(sm[r]);
-                        xi = xuse++;
-                        xsend<THREADS, R>(xch, xbar, C, rank, xi, zero, sm);
-                        if (!agree(xwait(xbar, xi, &st->status, p.suspend_ns))) {
-                            alive = false;
-                            break;
-                        }
-                        release(pb);  // every warp has finished reading batch pb's stage
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            const float Sr = slot_sum<THREADS, R>(xch, xi % kXSlots, C, r);
-                            anew[r] = -(M2[r] + log2f(Sr)) * kLn2;
-                            wr[r] = (M2[r] == -INFINITY) ? 0.f : ex2(M2[r] + anew[r] * kLog2e);
-                            if (r < rows) {
-                                const float2 w2 = make_float2(wr[r], wr[r]);
-#pragma unroll
-                                for (int h = 0; h < H; ++h) acc[h] = __ffma2_rn(e[r][h], w2, acc[h]);
-                            }
-                        }
-                    }
-                    if (rank == 0 && tid < rows) {
-                        float v = anew[0];
-#pragma unroll
-                        for (int r = 1; r < R; ++r)
-                            if (tid == r) v = anew[r];
-                        p.a[r0 + tid] = v;
-                    }
-                }
-                x_prev = x_cur;
-            }
-            bt = waited;
-        }
-    } else
     for (; bt < nbatch; ++bt) {
         const int s = bt % p.stages;
         if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status, p.suspend_ns))) {
@@ -874,17 +610,307 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
         for (int b = bt; b < issued; ++b)
             if (!mbar_wait(&full[b % p.stages], static_cast<uint32_t>((b / p.stages) & 1), &st->status)) break;
     }
-    // Tensor memory goes back once every warp's TMEM accesses have completed.
-    if constexpr (PIPE) {
-        if (pipelined) tmem_wait_st();
-        tmem_fence_before_sync();
-        __syncthreads();
-        tmem_fence_after_sync();
-        if (pipelined && (tid >> 5) == 0) tmem_dealloc(tmem_slot, TCOLS);
-    }
+
     // No CTA leaves while a peer may still send into its shared memory; the
     // non-aligned form tolerates threads that left the batch loop early.
     cluster_sync_any();
+}
+
+// ---------------------------------------------------------------------------
+// Row-owned 16-bit sweep (n <= 32768): one 512-thread CTA per SM walks a block
+// of whole rows, so the row normaliser is a CTA barrier instead of a cluster
+// exchange, and each thread keeps the running column sums of its EPT columns
+// in tensor memory (TMEM lane 32 (warp % 4) + lane, columns (warp / 4) EPT ..).
+// Rows stream through shared memory in segments of up to 16384 elements
+// (32 KB) with bulk copies; the column duals (b log2 e) of the whole row sit in
+// shared memory.  Same arithmetic as sweep_kernel: fast path against the
+// absorbed frame (one barrier per row), exact max-stabilised path (two more
+// barriers) for exact sweeps and for rows whose sum leaves (1e-30, 1e30).
+// Waits are bounded; a timed-out wait is agreed at the next barrier
+// (__syncthreads_and), so every thread leaves the row loop together.
+constexpr int kRowThreads = 512;
+constexpr int kRowWarps = kRowThreads / 32;
+constexpr int kRowSeg = 16384;  // elements per stage segment
+
+struct RowArgs {
+    const void* L;
+    long long ld;
+    int n;
+    int n_copy;          // columns copied per row (multiple of 8)
+    int rows_per_cta;
+    int stages;
+    unsigned suspend_ns;
+    const float* b_buf;  // [2][n_pad]
+    const float* logcs;
+    float* b_buf_w;
+    float* a;
+    float* partials;     // [ctas][n_pad]
+    long long n_pad;
+    SolveState* st;
+};
+
+template <typename T, int EPT>
+__global__ void __launch_bounds__(kRowThreads, 1) row_sweep_kernel(const RowArgs p) {
+    constexpr int EPS = EPT > 32 ? 32 : EPT;  // elements per thread per segment
+    constexpr int NSEG = EPT / EPS;
+    constexpr int G = EPS / 8;                // 16-byte chunks per thread per segment
+    constexpr int SEG = kRowThreads * EPS;    // elements per segment
+    constexpr int H = EPT / 2;
+    constexpr uint32_t TCOLS = 4 * EPT;
+    static_assert(SEG <= kRowSeg, "segment larger than a stage");
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t full[kMaxStages];
+    __shared__ float red_s[2][kRowWarps];
+    __shared__ float red_m[2][kRowWarps];
+    __shared__ uint32_t tmem_slot;
+
+    SolveState* st = p.st;
+    if (*reinterpret_cast<volatile int*>(&st->done)) return;  // uniform
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = p.n;
+    constexpr int COVER = kRowThreads * EPT;  // columns the threads cover (>= n)
+    float* b_s = reinterpret_cast<float*>(smem);
+    unsigned char* stage_base = smem + static_cast<size_t>(COVER) * 4;
+    const size_t stage_bytes = static_cast<size_t>(SEG) * sizeof(T);
+    const int row_begin = blockIdx.x * p.rows_per_cta;
+    const int row_end = min(n, row_begin + p.rows_per_cta);
+    const int nrows = max(0, row_end - row_begin);
+    const int units = nrows * NSEG;
+    const int t = st->it;
+    const float omega = static_cast<float>(st->omega);
+    const bool momentum = omega != 1.0f;
+    const bool exact_only = st->exact_next != 0 || momentum;  // uniform
+    const float* b_prev = p.b_buf + ((t - 1) & 1) * p.n_pad;
+    float* b_out = p.b_buf_w + (t & 1) * p.n_pad;
+    const float2 log2e2 = make_float2(kLog2e, kLog2e);
+
+    // column duals of this sweep, b = b_prev - w log(colsum_prev), kept as b log2 e;
+    // -inf past n, so those columns contribute exactly 0
+    for (int j = tid; j < COVER; j += kRowThreads) {
+        float b = -INFINITY;
+        if (j < n) {
+            const float bj = b_prev[j] - omega * p.logcs[j];
+            if (blockIdx.x == 0) b_out[j] = bj;
+            b = bj * kLog2e;
+        }
+        b_s[j] = b;
+    }
+    // stage memory starts finite (columns past n_copy are never copied)
+    for (size_t k = tid; k < static_cast<size_t>(p.stages) * SEG; k += kRowThreads)
+        reinterpret_cast<T*>(stage_base)[k] = from_float<T>(0.f);
+    if (tid == 0) {
+        for (int s = 0; s < p.stages; ++s) mbar_init(&full[s], 1);
+        fence_mbarrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&tmem_slot, TCOLS);
+        tmem_relinquish();
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tcol = tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) +
+                          static_cast<uint32_t>((warp >> 2) * EPT);
+    {
+        float z[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) z[k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < EPT / 16; ++k) tmem_st16(tcol + 16 * k, z);
+    }
+
+    auto issue = [&](int u) {
+        const int s = u % p.stages;
+        const int row = row_begin + u / NSEG;
+        const int seg = u % NSEG;
+        const int cols = min(SEG, p.n_copy - seg * SEG);
+        const uint32_t bytes = cols > 0 ? static_cast<uint32_t>(cols) * sizeof(T) : 0u;
+        mbar_arrive_expect_tx(&full[s], bytes);
+        if (bytes > 0)
+            bulk_load(stage_base + s * stage_bytes,
+                      static_cast<const T*>(p.L) + static_cast<size_t>(row) * p.ld + static_cast<size_t>(seg) * SEG,
+                      bytes, &full[s]);
+    };
+    int issued = 0;
+    if (tid == 0) {
+        fence_proxy_async_smem();  // the zero fill above precedes the copies
+        issued = min(p.stages, units);
+        for (int u = 0; u < issued; ++u) issue(u);
+    }
+    auto release = [&](int r) {
+        if (tid == 0) {
+            fence_proxy_async_smem();
+            for (int s = 0; s < NSEG; ++s) {
+                const int u = r * NSEG + s + p.stages;
+                if (u < units) {
+                    issue(u);
+                    ++issued;
+                }
+            }
+        }
+    };
+    auto b2_at = [&](int c, float2* b2) {
+        const float4 lo = *reinterpret_cast<const float4*>(b_s + c);
+        const float4 hi = *reinterpret_cast<const float4*>(b_s + c + 4);
+        b2[0] = make_float2(lo.x, lo.y);
+        b2[1] = make_float2(lo.z, lo.w);
+        b2[2] = make_float2(hi.x, hi.y);
+        b2[3] = make_float2(hi.z, hi.w);
+    };
+
+    bool alive = true;
+    int r = 0;
+    for (; r < nrows; ++r) {
+        const int row = row_begin + r;
+        const int par = r & 1;
+        bool ok = true;
+        float2 y[H];
+        float anew = 0.f, wr = 0.f;
+        bool fast_ok = false;
+        if (!exact_only) {
+            // ---- fast path: 2^(L log2e + b) against the absorbed frame
+            float2 s2 = make_float2(0.f, 0.f), t2 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int sg = 0; sg < NSEG; ++sg) {
+                const int u = r * NSEG + sg;
+                ok = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
+                               p.suspend_ns) && ok;
+                const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    const int cl = (g * kRowThreads + tid) * 8;
+                    float2 b2[4], v2[4];
+                    b2_at(sg * SEG + cl, b2);
+                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 e = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[q]));
+                        y[(sg * EPS + g * 8) / 2 + q] = e;
+                        if (q & 1)
+                            t2 = __fadd2_rn(t2, e);
+                        else
+                            s2 = __fadd2_rn(s2, e);
+                    }
+                }
+            }
+            const float2 u2 = __fadd2_rn(s2, t2);
+            const float part = warp_sum(u2.x + u2.y);
+            if (lane == 0) red_s[par][warp] = part;
+            if (!__syncthreads_and(ok)) {
+                alive = false;
+                break;
+            }
+            float S = 0.f;
+#pragma unroll
+            for (int w = 0; w < kRowWarps; ++w) S += red_s[par][w];
+            fast_ok = S > 1e-30f && S < 1e30f;  // uniform
+            if (fast_ok) {
+                release(r);
+                anew = -__log2f(S) * kLn2;
+                wr = __frcp_rn(S);
+            }
+        }
+        if (!fast_ok) {
+            // ---- exact path: row maximum, then the exponentials relative to it
+            float mx = -INFINITY;
+#pragma unroll
+            for (int sg = 0; sg < NSEG; ++sg) {
+                const int u = r * NSEG + sg;
+                if (exact_only)
+                    ok = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
+                                   p.suspend_ns) && ok;
+                const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    const int cl = (g * kRowThreads + tid) * 8;
+                    float2 b2[4], v2[4];
+                    b2_at(sg * SEG + cl, b2);
+                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 x = __ffma2_rn(v2[q], log2e2, b2[q]);
+                        y[(sg * EPS + g * 8) / 2 + q] = x;
+                        mx = fmaxf(mx, fmaxf(x.x, x.y));
+                    }
+                }
+            }
+            mx = warp_max(mx);
+            if (lane == 0) red_m[par][warp] = mx;
+            if (!__syncthreads_and(ok)) {
+                alive = false;
+                break;
+            }
+            float M2 = -INFINITY;
+#pragma unroll
+            for (int w = 0; w < kRowWarps; ++w) M2 = fmaxf(M2, red_m[par][w]);
+            const float base = (M2 == -INFINITY) ? 0.f : M2;
+            const float2 nb = make_float2(-base, -base);
+            float2 ss = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int h = 0; h < H; ++h) {
+                y[h] = ex2_pair(__fadd2_rn(y[h], nb));
+                ss = __fadd2_rn(ss, y[h]);
+            }
+            const float part = warp_sum(ss.x + ss.y);
+            if (lane == 0) red_s[par][warp] = part;
+            __syncthreads();
+            release(r);
+            float S = 0.f;
+#pragma unroll
+            for (int w = 0; w < kRowWarps; ++w) S += red_s[par][w];
+            const float lse = (M2 + log2f(S)) * kLn2;
+            anew = momentum ? (1.f - omega) * p.a[row] - omega * lse : -lse;
+            wr = (M2 == -INFINITY) ? 0.f : ex2(M2 + anew * kLog2e);
+            if (momentum) __syncthreads();  // every thread has read a[row] before it is overwritten
+        }
+        if (tid == 0) p.a[row] = anew;
+        // column sums of the row-normalised plan, accumulated in TMEM
+        const float2 w2 = make_float2(wr, wr);
+#pragma unroll
+        for (int k = 0; k < EPT / 16; ++k) {
+            float acc[16];
+            tmem_ld16(tcol + 16 * k, acc);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float2 a2 = __ffma2_rn(y[8 * k + q], w2, make_float2(acc[2 * q], acc[2 * q + 1]));
+                acc[2 * q] = a2.x;
+                acc[2 * q + 1] = a2.y;
+            }
+            tmem_st16(tcol + 16 * k, acc);
+        }
+    }
+
+    // per-CTA column sums -> partials[cta][col]
+    tmem_wait_st();
+    float* prow = p.partials + static_cast<size_t>(blockIdx.x) * p.n_pad;
+#pragma unroll
+    for (int k = 0; k < EPT / 16; ++k) {
+        float acc[16];
+        tmem_ld16(tcol + 16 * k, acc);
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int e = 16 * k + 8 * half;  // element index: segment e / EPS, chunk (e % EPS) / 8
+            const int c = (e / EPS) * SEG + (((e % EPS) / 8) * kRowThreads + tid) * 8;
+            const float* src = acc + 8 * half;
+            if (c + 8 <= n) {
+                *reinterpret_cast<float4*>(prow + c) = make_float4(src[0], src[1], src[2], src[3]);
+                *reinterpret_cast<float4*>(prow + c + 4) = make_float4(src[4], src[5], src[6], src[7]);
+            } else {
+                for (int q = 0; q < 8; ++q)
+                    if (c + q < n) prow[c + q] = src[q];
+            }
+        }
+    }
+    // a timed-out wait may leave copies in flight: wait for them (bounded)
+    if (!alive && tid == 0) {
+        for (int u = r * NSEG; u < issued; ++u)
+            if (!mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status)) break;
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    if (warp == 0) tmem_dealloc(tmem_slot, TCOLS);
 }
 
 // Reduce the per-cluster column sums (FP64), write log(colsum), decide.
@@ -1143,12 +1169,6 @@ unsigned suspend_hint() {
     return static_cast<unsigned>(v < 0 ? 0 : (v > 1000000 ? 1000000 : v));
 }
 
-// TMEM-pipelined 16-bit fast sweeps (FUGAL_SWEEP_PIPELINE=1 turns them on).
-int pipeline_choice() {
-    const char* e = getenv("FUGAL_SWEEP_PIPELINE");
-    return (e != nullptr && atoi(e) != 0) ? 1 : 0;
-}
-
 // Launch shapes: (threads per CTA, columns per thread).  Rows per batch are
 // 32 / columns-per-thread, so a thread always holds 32 exponentials.
 constexpr int rows_per_batch(int kpt) { return 32 / kpt; }
@@ -1290,6 +1310,53 @@ fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_oc
     return fail(FUGAL_UNSUPPORTED, "sinkhorn: could not fit the row-dual staging for n = %lld", (long long)n);
 }
 
+// Row-owned 16-bit sweep plan (row_sweep_kernel): used for 16-bit sweeps when
+// the padded row fits 32768 columns; FUGAL_ROW_SWEEP=0 selects the cluster
+// kernel instead.
+struct RowPlan {
+    bool use = false;
+    int ept = 0;
+    int ctas = 0;
+    int rows_per_cta = 0;
+    int stages = 0;
+    size_t smem = 0;
+    KernelFn fn = nullptr;
+};
+
+using RowKernelFn = void (*)(const RowArgs);
+
+RowKernelFn row_kernel_for(int dt, int ept) {
+    if (dt == FUGAL_BF16)
+        return ept == 16 ? row_sweep_kernel<__nv_bfloat16, 16>
+                         : (ept == 32 ? row_sweep_kernel<__nv_bfloat16, 32> : row_sweep_kernel<__nv_bfloat16, 64>);
+    return ept == 16 ? row_sweep_kernel<__half, 16> : (ept == 32 ? row_sweep_kernel<__half, 32> : row_sweep_kernel<__half, 64>);
+}
+
+fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool set_attributes) {
+    rp = RowPlan{};
+    if (dt == FUGAL_F32) return FUGAL_OK;
+    const char* e = getenv("FUGAL_ROW_SWEEP");
+    if (e != nullptr && atoi(e) == 0) return FUGAL_OK;
+    if (n_pad > 32768) return FUGAL_OK;
+    rp.ept = n_pad <= 8192 ? 16 : (n_pad <= 16384 ? 32 : 64);
+    const size_t stage_bytes = static_cast<size_t>(kRowThreads) * std::min(rp.ept, 32) * 2;
+    const size_t fixed = static_cast<size_t>(kRowThreads) * rp.ept * 4;  // column duals of every covered column
+    const int64_t room = static_cast<int64_t>(max_smem_optin()) - 1024 - static_cast<int64_t>(fixed);
+    rp.stages = static_cast<int>(std::min<int64_t>(kMaxStages, room / static_cast<int64_t>(stage_bytes)));
+    if (rp.stages < 2) return FUGAL_OK;
+    rp.smem = fixed + rp.stages * stage_bytes;
+    const int ctas = static_cast<int>(std::min<int64_t>(sm_count(), n));
+    rp.rows_per_cta = static_cast<int>((n + ctas - 1) / ctas);
+    rp.ctas = static_cast<int>((n + rp.rows_per_cta - 1) / rp.rows_per_cta);
+    if (set_attributes) {
+        RowKernelFn fn = row_kernel_for(dt, rp.ept);
+        FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp.smem),
+                             "sinkhorn: row sweep shared memory"));
+    }
+    rp.use = true;
+    return FUGAL_OK;
+}
+
 constexpr int kColThreads = 256;
 
 int colpass_chunks(int64_t n) {
@@ -1387,6 +1454,17 @@ extern "C" fugal_status fugal_sinkhorn_plan_info(int64_t n, int stream_dtype, in
     if (info == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_plan_info: null output");
     if (stream_dtype < FUGAL_F32 || stream_dtype > FUGAL_F16)
         return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_plan_info: bad stream dtype");
+    RowPlan rp;
+    FUGAL_TRY(make_row_plan(n, stream_dtype, static_cast<int64_t>(align_up(static_cast<size_t>(n), 64)), rp, false));
+    if (rp.use) {  // row-owned sweep: one CTA per SM, no cluster
+        info[0] = kRowThreads;
+        info[1] = 1;
+        info[2] = rp.ctas;
+        info[3] = rp.stages;
+        info[4] = static_cast<int32_t>(rp.smem);
+        info[5] = 1;
+        return FUGAL_OK;
+    }
     SweepPlan pl;
     FUGAL_TRY(make_plan(n, stream_dtype, 0, pl, true));
     info[0] = pl.threads;
@@ -1427,12 +1505,15 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
                     w.bytes);
 
     SweepPlan plan32, plan16, plan_abs;
+    RowPlan rowplan;
     FUGAL_TRY(make_plan(n, FUGAL_F32, 0, plan32, true));
+    if (use16) FUGAL_TRY(make_row_plan(n, p.stream_dtype, w.n_pad, rowplan, true));
     if (use16) {
-        FUGAL_TRY(make_plan(n, p.stream_dtype, 0, plan16, true));
+        if (!rowplan.use) FUGAL_TRY(make_plan(n, p.stream_dtype, 0, plan16, true));
         FUGAL_TRY(make_plan(n, FUGAL_F32, p.stream_dtype == FUGAL_BF16 ? 1 : 2, plan_abs, true));
     }
-    if (plan32.clusters > prow || (use16 && (plan16.clusters > prow || plan_abs.clusters > prow)))
+    if (plan32.clusters > prow || (use16 && (plan16.clusters > prow || plan_abs.clusters > prow)) ||
+        rowplan.ctas > prow)
         return fail(FUGAL_UNSUPPORTED, "fugal_sinkhorn_solve: more clusters than partial rows");
 
     FrameArgs frame{use16 ? 1 : 0, use16 ? p.fp32_warmup_sweeps : 0, use16 ? p.reabsorb_every : 1,
@@ -1473,7 +1554,6 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         a.rows_per_cluster = pl.rows_per_cluster;
         a.rows_pad = pl.rows_pad;
         a.suspend_ns = suspend_hint();
-        a.pipeline = pipeline_choice();
         a.stages = pl.stages;
         a.b_buf = w.b_buf;
         a.b_buf_w = w.b_buf;
@@ -1539,6 +1619,28 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
             status = launch_sweep(plan_abs, kernel_for(plan_abs.threads, plan_abs.kpt, FUGAL_F32, p.stream_dtype == FUGAL_BF16 ? 1 : 2),
                                   a, stream, FUGAL_KERNEL_ABSORB);
             if (status == FUGAL_OK) status = finalize(plan_abs.clusters);
+        } else if (rowplan.use) {
+            RowArgs ra{};
+            ra.L = p.cost16;
+            ra.ld = p.ld16;
+            ra.n = static_cast<int>(n);
+            ra.n_copy = static_cast<int>((n + 7) / 8 * 8);
+            ra.rows_per_cta = rowplan.rows_per_cta;
+            ra.stages = rowplan.stages;
+            ra.suspend_ns = suspend_hint();
+            ra.b_buf = w.b_buf;
+            ra.logcs = w.logcs;
+            ra.b_buf_w = w.b_buf;
+            ra.a = w.a;
+            ra.partials = w.partials;
+            ra.n_pad = w.n_pad;
+            ra.st = w.st;
+            {
+                LaunchScope scope(FUGAL_KERNEL_SWEEP, stream);
+                row_kernel_for(p.stream_dtype, rowplan.ept)<<<rowplan.ctas, kRowThreads, rowplan.smem, stream>>>(ra);
+                status = launch_check("sinkhorn: row sweep");
+            }
+            if (status == FUGAL_OK) status = finalize(rowplan.ctas);
         } else {
             SweepArgs a = sweep_args(plan16, p.cost16, p.ld16, nullptr, nullptr);
             status = launch_sweep(plan16, kernel_for(plan16.threads, plan16.kpt, p.stream_dtype, 0), a, stream, FUGAL_KERNEL_SWEEP);

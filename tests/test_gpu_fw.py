@@ -149,9 +149,12 @@ def test_sinkhorn_momentum_matches_oracle():
     np.testing.assert_allclose(_plan(C, u, v, 0.05), _plan(C, ref.u, ref.v, 0.05), atol=2e-4)
 
 
+@pytest.mark.parametrize("kernel", ["rows", "cluster"])
 @pytest.mark.parametrize("dtype,tol", [(torch.bfloat16, 1e-2), (torch.float16, 2e-3)])
 @pytest.mark.parametrize("n", [300, 3000, 9000])
-def test_sinkhorn_reduced_precision_stream(dtype, tol, n):
+def test_sinkhorn_reduced_precision_stream(dtype, tol, n, kernel, monkeypatch):
+    if kernel == "cluster":
+        monkeypatch.setenv("FUGAL_ROW_SWEEP", "0")
     rng = np.random.default_rng(11)
     C = (rng.random((n, n)) * 4).astype(np.float32).astype(np.float64)
     zero = np.zeros(n)
@@ -164,6 +167,63 @@ def test_sinkhorn_reduced_precision_stream(dtype, tol, n):
     P, R = _plan(C, u, v, reg), _plan(C, ref.u, ref.v, reg)
     np.testing.assert_allclose(P, R, atol=tol)
     np.testing.assert_allclose(P.sum(axis=1), 1.0, atol=1e-4)  # rows exact after the FP32 polish sweep
+
+
+def _solve_device(Ct, reg, max_iter, stream_dtype=None, polish=1, warmup=3, every=4):
+    """Zero-start solve of the device cost Ct (n x n FP32, torch): (u, v) FP64 numpy."""
+    from cugal_b200 import _native as N
+    from cugal_b200.config import Config, SinkhornMethod
+    from cugal_b200.sinkhorn import SinkhornSolver, padded_ld
+    n = Ct.shape[0]
+    cfg = Config(device="cuda", dtype=torch.float32, sinkhorn_method=SinkhornMethod.LOG,
+                 sinkhorn_regularization=reg, sinkhorn_iterations=max_iter, sinkhorn_threshold=0.0,
+                 sinkhorn_eval_freq=10, stream_dtype=stream_dtype, polish_sweeps=polish, fp32_warmup_sweeps=warmup,
+                 reabsorb_every=every)
+    solver = SinkhornSolver(n, cfg, "cuda")
+    cost = torch.zeros((n, padded_ld(n)), dtype=torch.float32, device="cuda")
+    cost[:, :n] = Ct / -reg
+    du = torch.empty(n, dtype=torch.float32, device="cuda")
+    dv = torch.empty(n, dtype=torch.float32, device="cuda")
+    solver.solve(cost, du, dv, None)
+    torch.cuda.synchronize()
+    del solver, cost
+    return du.cpu().numpy().astype(np.float64), dv.cpu().numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("n", [17000, 20000, 32768])
+def test_row_sweep_matches_cluster_sweep_and_fp32(n, monkeypatch):
+    """16-bit solves with the row-owned sweep (two row segments, padded columns)
+    against the cluster sweep and the FP32 stream on the same problem."""
+    g = torch.Generator(device="cuda").manual_seed(n)
+    Ct = torch.rand((n, n), generator=g, device="cuda") * 4
+    reg = 0.05
+    u_r, v_r = _solve_device(Ct, reg, 12, stream_dtype=torch.bfloat16)
+    monkeypatch.setenv("FUGAL_ROW_SWEEP", "0")
+    u_c, v_c = _solve_device(Ct, reg, 12, stream_dtype=torch.bfloat16)
+    u_f, v_f = _solve_device(Ct, reg, 12)
+    rows = np.random.default_rng(n).choice(n, 64, replace=False)
+    Cs = Ct[torch.tensor(rows, device="cuda")].double().cpu().numpy()
+    del Ct
+    torch.cuda.empty_cache()
+    P_r = np.exp(-Cs / reg + u_r[rows, None] + v_r[None, :])
+    P_c = np.exp(-Cs / reg + u_c[rows, None] + v_c[None, :])
+    P_f = np.exp(-Cs / reg + u_f[rows, None] + v_f[None, :])
+    np.testing.assert_allclose(P_r, P_c, atol=1e-2)
+    np.testing.assert_allclose(P_r, P_f, atol=1e-2)
+    np.testing.assert_allclose(P_r.sum(axis=1), 1.0, atol=1e-3)
+
+
+def test_row_sweep_momentum_matches_oracle():
+    n = 3000
+    rng = np.random.default_rng(21)
+    C = (rng.random((n, n)) * 4).astype(np.float32).astype(np.float64)
+    zero = np.zeros(n)
+    reg = 0.05
+    ref = O.sinkhorn_log_solve(C, zero, zero, reg, 60, 0.0, 10, 20)
+    u, v, prof = _solve_gpu(C, zero, zero, reg, 60, 0.0, 10, mstart=20, stream_dtype=torch.bfloat16, polish=1,
+                            warmup=3, every=20)
+    assert prof.iteration_count == 60
+    np.testing.assert_allclose(_plan(C, u, v, reg), _plan(C, ref.u, ref.v, reg), atol=1e-2)
 
 
 def test_update_matches_oracle():
