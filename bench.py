@@ -183,12 +183,22 @@ def load_peak():
 
 
 def traffic_per_launch(n: int, ld: int):
-    """DRAM bytes per 16-bit sweep launch from the committed ncu summary (scaled by rows x ld), or None."""
-    f = ROOT / "profiles" / "sweep_bf16_traffic.json"
+    """DRAM bytes per 16-bit sweep launch from the committed ncu summary
+    (profiles/row_sweep_bf16_n16384.md, `key: value` lines), scaled by the
+    elements of the cost copy (traffic grows with rows x ld), or None."""
+    f = ROOT / "profiles" / "row_sweep_bf16_n16384.md"
     if not f.exists():
         return None
-    d = json.loads(f.read_text())
-    return d["dram_bytes_per_launch"] * (n * ld) / (d["n"] * d["ld"])
+    vals = {}
+    for line in f.read_text().splitlines():
+        if line.startswith("- ") and ": " in line:
+            k, v = line[2:].split(": ", 1)
+            vals[k.strip()] = v.strip()
+    try:
+        per = float(vals["dram_bytes_per_launch"])
+        return per * (n * ld) / (float(vals["n"]) * float(vals["ld"]))
+    except (KeyError, ValueError):
+        return None
 
 
 def executed_sweeps(iteration_counts, config) -> dict:
