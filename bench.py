@@ -16,8 +16,8 @@ the alignment path has no exchange step), timing is the max over ranks and
 `value` is seconds per step, i.e. per N alignments (weak scaling).
 
 The JSON line also carries the roofline of the dominant kernel (the BF16 sweep:
-algorithmic bytes = one read of the n x ld 16-bit cost per launch, averaged over
-the launches of the timed region with CUDA events on the launch stream), the
+algorithmic bytes = one read of the n x ld 16-bit cost per sweep that ran, over
+the CUDA-event time of all its launches in the timed region), the
 host CPU baseline (the reference's FP64 CPU Sinkhorn iteration timed on a block
 of rows, extrapolated), SM clocks sampled during the timed region, and the
 number of this library's kernel launches in the timed region.
@@ -144,8 +144,8 @@ def cpu_sweep_seconds(n: int, budget_s: float) -> tuple[float, int, str]:
 
     Restates cugal/sinkhorn.py:108-111 (torch FP64: a column logsumexp and a row
     logsumexp over K + potentials) on a block of rows of an n-column cost, all
-    host threads, and scales the per-row time to n rows.  Uses the oracle's
-    module only for its shapes; the arithmetic is torch's, as in the reference."""
+    host threads, and scales the per-row time to n rows; the arithmetic is
+    torch's, as in the reference."""
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
     rows = max(64, min(n, 2048))
@@ -252,6 +252,8 @@ def run_reference(args):
     n = args.n or w.n
     iters = args.iter_count or w.iter_count
     solves = iters * 10
+    # The reference's convergence check mutates K (cugal/sinkhorn.py:67-74) and never
+    # passes, so its solve runs to sinkhorn_iterations (500) every time.
     sweeps = args.sinkhorn_iterations or 500
     vals = []
     for _ in range(args.warmup):
