@@ -1504,7 +1504,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         return fail(FUGAL_WORKSPACE_TOO_SMALL, "fugal_sinkhorn_solve: workspace %zu < %zu bytes", workspace_bytes,
                     w.bytes);
 
-    SweepPlan plan32, plan16, plan_abs;
+    SweepPlan plan32{}, plan16{}, plan_abs{};
     RowPlan rowplan;
     FUGAL_TRY(make_plan(n, FUGAL_F32, 0, plan32, true));
     if (use16) FUGAL_TRY(make_row_plan(n, p.stream_dtype, w.n_pad, rowplan, true));
