@@ -628,8 +628,6 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
 // barriers) for exact sweeps and for rows whose sum leaves (1e-30, 1e30).
 // Waits are bounded; a timed-out wait is agreed at the next barrier
 // (__syncthreads_and), so every thread leaves the row loop together.
-constexpr int kRowThreads = 512;
-constexpr int kRowWarps = kRowThreads / 32;
 constexpr int kRowSeg = 16384;  // elements per stage segment
 
 struct RowArgs {
@@ -649,14 +647,17 @@ struct RowArgs {
     SolveState* st;
 };
 
-template <typename T, int EPT>
-__global__ void __launch_bounds__(kRowThreads, 1) row_sweep_kernel(const RowArgs p) {
-    constexpr int EPS = EPT > 32 ? 32 : EPT;  // elements per thread per segment
+template <typename T, int EPT, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) {
+    constexpr int kRowThreads = THREADS;
+    constexpr int kRowWarps = THREADS / 32;
+    constexpr int EPS = EPT > kRowSeg / THREADS ? kRowSeg / THREADS : EPT;  // elements per thread per segment
     constexpr int NSEG = EPT / EPS;
     constexpr int G = EPS / 8;                // 16-byte chunks per thread per segment
     constexpr int SEG = kRowThreads * EPS;    // elements per segment
     constexpr int H = EPT / 2;
-    constexpr uint32_t TCOLS = 4 * EPT;
+    constexpr uint32_t TCOLS = (THREADS / 128) * EPT;
+    static_assert(EPT % 16 == 0 && EPS % 8 == 0, "16-column TMEM chunks, 8-element loads");
     static_assert(SEG <= kRowSeg, "segment larger than a stage");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full[kMaxStages];
@@ -1315,6 +1316,7 @@ fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_oc
 // kernel instead.
 struct RowPlan {
     bool use = false;
+    int threads = 512;
     int ept = 0;
     int ctas = 0;
     int rows_per_cta = 0;
@@ -1325,11 +1327,24 @@ struct RowPlan {
 
 using RowKernelFn = void (*)(const RowArgs);
 
-RowKernelFn row_kernel_for(int dt, int ept) {
-    if (dt == FUGAL_BF16)
-        return ept == 16 ? row_sweep_kernel<__nv_bfloat16, 16>
-                         : (ept == 32 ? row_sweep_kernel<__nv_bfloat16, 32> : row_sweep_kernel<__nv_bfloat16, 64>);
-    return ept == 16 ? row_sweep_kernel<__half, 16> : (ept == 32 ? row_sweep_kernel<__half, 32> : row_sweep_kernel<__half, 64>);
+template <typename T>
+RowKernelFn row_kernel_typed(int ept, int threads) {
+    if (threads == 1024) return ept == 16 ? row_sweep_kernel<T, 16, 1024> : row_sweep_kernel<T, 32, 1024>;
+    return ept == 16 ? row_sweep_kernel<T, 16, 512>
+                     : (ept == 32 ? row_sweep_kernel<T, 32, 512> : row_sweep_kernel<T, 64, 512>);
+}
+
+RowKernelFn row_kernel_for(int dt, int ept, int threads) {
+    return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16>(ept, threads) : row_kernel_typed<__half>(ept, threads);
+}
+
+// Threads per row-sweep CTA: 1024 (two warps per TMEM lane quarter more, twice
+// the warps to hide latency) when the padded row exceeds 8192 columns, else 512;
+// FUGAL_ROW_THREADS=512 or 1024 overrides.
+int row_threads_for(int64_t n_pad) {
+    const char* e = getenv("FUGAL_ROW_THREADS");
+    if (e != nullptr && (atoi(e) == 512 || atoi(e) == 1024)) return n_pad <= 8192 ? 512 : atoi(e);
+    return n_pad <= 8192 ? 512 : 1024;
 }
 
 fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool set_attributes) {
@@ -1338,9 +1353,11 @@ fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool s
     const char* e = getenv("FUGAL_ROW_SWEEP");
     if (e != nullptr && atoi(e) == 0) return FUGAL_OK;
     if (n_pad > 32768) return FUGAL_OK;
-    rp.ept = n_pad <= 8192 ? 16 : (n_pad <= 16384 ? 32 : 64);
-    const size_t stage_bytes = static_cast<size_t>(kRowThreads) * std::min(rp.ept, 32) * 2;
-    const size_t fixed = static_cast<size_t>(kRowThreads) * rp.ept * 4;  // column duals of every covered column
+    rp.threads = row_threads_for(n_pad);
+    rp.ept = static_cast<int>((n_pad + rp.threads * 16 - 1) / (rp.threads * 16)) * 16;  // 16, 32 or 64
+    if (rp.ept == 48) rp.ept = 64;
+    const size_t stage_bytes = static_cast<size_t>(rp.threads) * std::min(rp.ept, kRowSeg / rp.threads) * 2;
+    const size_t fixed = static_cast<size_t>(rp.threads) * rp.ept * 4;  // column duals of every covered column
     const int64_t room = static_cast<int64_t>(max_smem_optin()) - 1024 - static_cast<int64_t>(fixed);
     rp.stages = static_cast<int>(std::min<int64_t>(kMaxStages, room / static_cast<int64_t>(stage_bytes)));
     if (rp.stages < 2) return FUGAL_OK;
@@ -1349,7 +1366,7 @@ fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool s
     rp.rows_per_cta = static_cast<int>((n + ctas - 1) / ctas);
     rp.ctas = static_cast<int>((n + rp.rows_per_cta - 1) / rp.rows_per_cta);
     if (set_attributes) {
-        RowKernelFn fn = row_kernel_for(dt, rp.ept);
+        RowKernelFn fn = row_kernel_for(dt, rp.ept, rp.threads);
         FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp.smem),
                              "sinkhorn: row sweep shared memory"));
     }
@@ -1457,7 +1474,7 @@ extern "C" fugal_status fugal_sinkhorn_plan_info(int64_t n, int stream_dtype, in
     RowPlan rp;
     FUGAL_TRY(make_row_plan(n, stream_dtype, static_cast<int64_t>(align_up(static_cast<size_t>(n), 64)), rp, false));
     if (rp.use) {  // row-owned sweep: one CTA per SM, no cluster
-        info[0] = kRowThreads;
+        info[0] = rp.threads;
         info[1] = 1;
         info[2] = rp.ctas;
         info[3] = rp.stages;
@@ -1637,7 +1654,8 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
             ra.st = w.st;
             {
                 LaunchScope scope(FUGAL_KERNEL_SWEEP, stream);
-                row_kernel_for(p.stream_dtype, rowplan.ept)<<<rowplan.ctas, kRowThreads, rowplan.smem, stream>>>(ra);
+                row_kernel_for(p.stream_dtype, rowplan.ept, rowplan.threads)<<<rowplan.ctas, rowplan.threads, rowplan.smem,
+                                                                               stream>>>(ra);
                 status = launch_check("sinkhorn: row sweep");
             }
             if (status == FUGAL_OK) status = finalize(rowplan.ctas);
