@@ -1338,13 +1338,14 @@ RowKernelFn row_kernel_for(int dt, int ept, int threads) {
     return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16>(ept, threads) : row_kernel_typed<__half>(ept, threads);
 }
 
-// Threads per row-sweep CTA: 1024 (two warps per TMEM lane quarter more, twice
-// the warps to hide latency) when the padded row exceeds 8192 columns, else 512;
-// FUGAL_ROW_THREADS=512 or 1024 overrides.
+// Threads per row-sweep CTA: 512 (measured faster than 1024 at n = 16384 and
+// 32768: 1024 threads halve the columns per thread, so the per-row reduction
+// and barrier cost more per element); FUGAL_ROW_THREADS=1024 selects the wider
+// CTA above 8192 columns.
 int row_threads_for(int64_t n_pad) {
     const char* e = getenv("FUGAL_ROW_THREADS");
-    if (e != nullptr && (atoi(e) == 512 || atoi(e) == 1024)) return n_pad <= 8192 ? 512 : atoi(e);
-    return n_pad <= 8192 ? 512 : 1024;
+    if (e != nullptr && atoi(e) == 1024 && n_pad > 8192) return 1024;
+    return 512;
 }
 
 fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool set_attributes) {
