@@ -236,18 +236,45 @@ def structural_objective(P: torch.Tensor, A: Adjacency, B: Adjacency):
 
 def tune_mu(A: Adjacency, B: Adjacency, D: torch.Tensor, config: Config, P0: torch.Tensor, mu0: float = 0.2,
             steps: int = 20, lr: float = 0.05, lam: float = 0.0):
-    """Gradient steps on mu: C(mu) = -2 A P0 B + mu D + lam (1 - 2 P0), P(mu) =
-    Sinkhorn(C(mu)), objective = structural_objective(P(mu)).  Returns the list of
-    (mu, objective, d objective / d mu)."""
+    """Gradient descent on mu: C(mu) = -2 A P0 B + mu D + lam (1 - 2 P0), P(mu) =
+    Sinkhorn(C(mu)) (converged plan, implicit adjoint), objective =
+    structural_objective(P(mu)).  Each step moves along the normalised negative
+    gradient with a backtracking (Armijo) line search that starts at twice the
+    last accepted length (first: ``lr``), so the objective never increases.
+    Returns one (mu, objective, d objective / d mu) per step."""
     base = (-2.0 * _APB.apply(P0, A, B) + lam * (1 - 2 * P0)).detach()
-    mu = torch.tensor(mu0, dtype=torch.float64, device=P0.device, requires_grad=True)
-    history = []
-    for _ in range(steps):
+
+    def evaluate(mu_val: float, grad: bool):
+        mu = torch.tensor(mu_val, dtype=torch.float64, device=P0.device, requires_grad=grad)
         C = base + mu.float() * D
         P = sinkhorn_plan(C, config)
         obj = structural_objective(P, A, B)
+        if not grad:
+            return float(obj.item()), 0.0
         (g,) = torch.autograd.grad(obj, mu)
-        history.append((float(mu.item()), float(obj.item()), float(g.item())))
-        with torch.no_grad():
-            mu -= lr * g / max(1.0, abs(float(g.item())))
+        return float(obj.item()), float(g.item())
+
+    mu_val = mu0
+    obj, g = evaluate(mu_val, True)
+    history = []
+    length = lr
+    for _ in range(steps):
+        history.append((mu_val, obj, g))
+        if g == 0.0:
+            continue
+        direction = -g / max(1.0, abs(g))
+        t = length
+        accepted = False
+        for _ in range(10):
+            cand = mu_val + t * direction
+            obj_c, _ = evaluate(cand, False)
+            if obj_c <= obj + 1e-4 * t * g * direction:
+                accepted = True
+                break
+            t *= 0.5
+        if not accepted:
+            continue  # no decrease along the gradient at this resolution: stay
+        mu_val = cand
+        obj, g = evaluate(mu_val, True)
+        length = 2.0 * t
     return history

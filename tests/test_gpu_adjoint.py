@@ -88,10 +88,12 @@ def test_tune_mu_runs_and_descends():
     rng = np.random.default_rng(5)
     D = torch.tensor(rng.random((n, n)) * 3, dtype=torch.float32, device="cuda")
     P0 = torch.full((n, n), 1.0 / n, device="cuda")
-    hist = tune_mu(A, B, D, _config(0.05, iters=3000, thr=1e-4), P0, mu0=0.2, steps=5, lr=0.05)
+    hist = tune_mu(A, B, D, _config(0.05, iters=3000, thr=1e-4), P0, mu0=0.2, steps=5, lr=0.1)
     assert len(hist) == 5
     assert all(np.isfinite(x) for row in hist for x in row)
     assert hist[-1][0] != hist[0][0]
+    objs = [row[1] for row in hist]
+    assert all(b <= a + 1e-3 * abs(a) for a, b in zip(objs, objs[1:]))  # line search: no increase
 
 
 @pytest.mark.parametrize("k,every", [(0, 10), (1, 7)])
