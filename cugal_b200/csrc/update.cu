@@ -26,15 +26,9 @@ inline dim3 ew_grid(int64_t n) {
 }
 
 // q = exp(L + u_i + v_j); P += alpha (q - P); gap += (q - P) * (-reg (L - U_i - V_j)).
-// Grid-stride over (row, 1024-column chunk) units, two units per step with all
-// their loads issued before the arithmetic (more bytes in flight per thread);
-// every block reduces its gap once at the end (one FP64 atomic per block).
-struct UpdUnit {
-    int i, j0;
-    bool full, valid;
-    float4 l4, p4, v4;
-};
-
+// Grid-stride over (row, 1024-column chunk) units, each thread one float4 of a
+// unit per step; every block reduces its gap once at the end (one FP64 atomic
+// per block instead of one per unit).
 __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict__ P, long long ldp,
                                                                const float* __restrict__ L, long long ldl,
                                                                const float* __restrict__ u,
@@ -47,53 +41,38 @@ __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict
     const int chunks = (n + kChunk - 1) / kChunk;
     const long long units = static_cast<long long>(n) * chunks;
     double g = 0.0;
-    auto load = [&](long long w, UpdUnit& x) {
-        x.valid = false;
-        if (w >= units) return;
-        x.i = static_cast<int>(w / chunks);
-        x.j0 = static_cast<int>(w % chunks) * kChunk + threadIdx.x * 4;
-        if (x.j0 >= n) return;
-        x.valid = true;
-        x.full = x.j0 + 4 <= n;
-        if (x.full) {
-            x.l4 = *reinterpret_cast<const float4*>(L + static_cast<size_t>(x.i) * ldl + x.j0);
-            x.p4 = *reinterpret_cast<const float4*>(P + static_cast<size_t>(x.i) * ldp + x.j0);
-            x.v4 = *reinterpret_cast<const float4*>(v + x.j0);
-        }
-    };
-    auto apply = [&](const UpdUnit& x) {
-        if (!x.valid) return;
-        const float ui = u[x.i];
-        const double Ui = U ? U[x.i] : 0.0;
-        float* prow = P + static_cast<size_t>(x.i) * ldp;
-        const float* lrow = L + static_cast<size_t>(x.i) * ldl;
-        if (x.full) {
-            const float lv[4] = {x.l4.x, x.l4.y, x.l4.z, x.l4.w};
-            const float vv[4] = {x.v4.x, x.v4.y, x.v4.z, x.v4.w};
-            float pv[4] = {x.p4.x, x.p4.y, x.p4.z, x.p4.w};
+    for (long long w = blockIdx.x; w < units; w += gridDim.x) {
+        const int i = static_cast<int>(w / chunks);
+        const int j0 = static_cast<int>(w % chunks) * kChunk + threadIdx.x * 4;
+        if (j0 >= n) continue;
+        const float ui = u[i];
+        const double Ui = U ? U[i] : 0.0;
+        float* prow = P + static_cast<size_t>(i) * ldp;
+        const float* lrow = L + static_cast<size_t>(i) * ldl;
+        if (j0 + 4 <= n) {
+            const float4 l4 = *reinterpret_cast<const float4*>(lrow + j0);
+            float4 p4 = *reinterpret_cast<float4*>(prow + j0);
+            const float4 v4 = *reinterpret_cast<const float4*>(v + j0);
+            const float lv[4] = {l4.x, l4.y, l4.z, l4.w};
+            const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
+            float pv[4] = {p4.x, p4.y, p4.z, p4.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const float diff = expf(lv[q] + ui + vv[q]) - pv[q];
-                const double C = -reg * (static_cast<double>(lv[q]) - Ui - (V ? V[x.j0 + q] : 0.0));
+                const double C = -reg * (static_cast<double>(lv[q]) - Ui - (V ? V[j0 + q] : 0.0));
                 g += static_cast<double>(diff) * C;
                 pv[q] = fmaf(alpha, diff, pv[q]);
             }
-            *reinterpret_cast<float4*>(prow + x.j0) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+            p4 = make_float4(pv[0], pv[1], pv[2], pv[3]);
+            *reinterpret_cast<float4*>(prow + j0) = p4;
         } else {
-            for (int j = x.j0; j < n; ++j) {
+            for (int j = j0; j < n; ++j) {
                 const float diff = expf(lrow[j] + ui + v[j]) - prow[j];
                 const double C = -reg * (static_cast<double>(lrow[j]) - Ui - (V ? V[j] : 0.0));
                 g += static_cast<double>(diff) * C;
                 prow[j] = fmaf(alpha, diff, prow[j]);
             }
         }
-    };
-    for (long long w = blockIdx.x; w < units; w += 2ll * gridDim.x) {
-        UpdUnit a, b;
-        load(w, a);
-        load(w + gridDim.x, b);
-        apply(a);
-        apply(b);
     }
     g = block_sum(g, red);
     if (threadIdx.x == 0) atomicAdd(gap, g);
