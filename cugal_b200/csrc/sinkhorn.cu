@@ -663,6 +663,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     __shared__ uint64_t full[kMaxStages];
     __shared__ __align__(16) float red_s[2][kRowWarps];
     __shared__ __align__(16) float red_m[2][kRowWarps];
+    __shared__ __align__(16) float2 red_pair[2][kRowWarps];
     __shared__ uint32_t tmem_slot;
 
     SolveState* st = p.st;
@@ -760,8 +761,102 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         b2[3] = make_float2(hi.z, hi.w);
     };
 
+    // Fast-path exponentials of local row rr (its stages waited for here):
+    // yy = 2^(L log2e + b) against the absorbed frame, s2 / t2 partial row sums.
+    auto row_fast = [&](int rr, float2(&yy)[H], float2& s2, float2& t2, bool& okk) {
+#pragma unroll
+        for (int sg = 0; sg < NSEG; ++sg) {
+            const int u = rr * NSEG + sg;
+            okk = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
+                            p.suspend_ns) && okk;
+            const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int cl = (g * kRowThreads + tid) * 8;
+                float2 b2[4], v2[4];
+                b2_at(sg * SEG + cl, b2);
+                Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float2 e = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[q]));
+                    yy[(sg * EPS + g * 8) / 2 + q] = e;
+                    if (q & 1)
+                        t2 = __fadd2_rn(t2, e);
+                    else
+                        s2 = __fadd2_rn(s2, e);
+                }
+            }
+        }
+    };
+
     bool alive = true;
     int r = 0;
+    // Rows in pairs (one-segment rows, fast path): both rows' exponentials stay in
+    // registers, so the two rows share one barrier, one read of the per-warp sums
+    // and one pass over the TMEM accumulators.  A pair with a row outside the fast
+    // path's range hands the rest of the sweep to the single-row loop below,
+    // which restarts at that pair (its stages are still held).
+    if constexpr (NSEG == 1 && EPT <= 32) {
+        if (!exact_only) {
+            for (; r < nrows; r += 2) {
+                const int nr = min(2, nrows - r);
+                const int par = (r >> 1) & 1;
+                bool ok = true;
+                float2 ya[H], yb[H];
+                float2 sa = make_float2(0.f, 0.f), ta = sa, sb = sa, tb = sa;
+                row_fast(r, ya, sa, ta, ok);
+                if (nr == 2) {
+                    row_fast(r + 1, yb, sb, tb, ok);
+                } else {
+#pragma unroll
+                    for (int h = 0; h < H; ++h) yb[h] = make_float2(0.f, 0.f);
+                }
+                const float2 ua = __fadd2_rn(sa, ta), ub = __fadd2_rn(sb, tb);
+                float pa = ua.x + ua.y, pb = ub.x + ub.y;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    pa += __shfl_xor_sync(0xffffffffu, pa, o);
+                    pb += __shfl_xor_sync(0xffffffffu, pb, o);
+                }
+                if (lane == 0) red_pair[par][warp] = make_float2(pa, pb);
+                if (!__syncthreads_and(ok)) {
+                    alive = false;
+                    break;
+                }
+                float SA = 0.f, SB = 0.f;
+#pragma unroll
+                for (int w = 0; w < kRowWarps; ++w) {
+                    const float2 q = red_pair[par][w];
+                    SA += q.x;
+                    SB += q.y;
+                }
+                const bool in_range = SA > 1e-30f && SA < 1e30f && (nr < 2 || (SB > 1e-30f && SB < 1e30f));
+                if (!in_range) break;  // uniform
+                release(r);
+                if (nr == 2) release(r + 1);
+                const float wa = __frcp_rn(SA), wb = nr == 2 ? __frcp_rn(SB) : 0.f;
+                if (tid == 0) {
+                    p.a[row_begin + r] = -__log2f(SA) * kLn2;
+                    if (nr == 2) p.a[row_begin + r + 1] = -__log2f(SB) * kLn2;
+                }
+                const float2 wa2 = make_float2(wa, wa), wb2 = make_float2(wb, wb);
+#pragma unroll
+                for (int k = 0; k < EPT / 16; ++k) {
+                    float acc[16];
+                    tmem_ld16(tcol + 16 * k, acc);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        float2 a2 = __ffma2_rn(ya[8 * k + q], wa2, make_float2(acc[2 * q], acc[2 * q + 1]));
+                        a2 = __ffma2_rn(yb[8 * k + q], wb2, a2);
+                        acc[2 * q] = a2.x;
+                        acc[2 * q + 1] = a2.y;
+                    }
+                    tmem_st16(tcol + 16 * k, acc);
+                }
+            }
+        }
+    }
+    if (alive)
     for (; r < nrows; ++r) {
         const int row = row_begin + r;
         const int par = r & 1;
@@ -772,29 +867,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         if (!exact_only) {
             // ---- fast path: 2^(L log2e + b) against the absorbed frame
             float2 s2 = make_float2(0.f, 0.f), t2 = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int sg = 0; sg < NSEG; ++sg) {
-                const int u = r * NSEG + sg;
-                ok = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
-                               p.suspend_ns) && ok;
-                const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
-#pragma unroll
-                for (int g = 0; g < G; ++g) {
-                    const int cl = (g * kRowThreads + tid) * 8;
-                    float2 b2[4], v2[4];
-                    b2_at(sg * SEG + cl, b2);
-                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float2 e = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[q]));
-                        y[(sg * EPS + g * 8) / 2 + q] = e;
-                        if (q & 1)
-                            t2 = __fadd2_rn(t2, e);
-                        else
-                            s2 = __fadd2_rn(s2, e);
-                    }
-                }
-            }
+            row_fast(r, y, s2, t2, ok);
             const float2 u2 = __fadd2_rn(s2, t2);
             const float part = warp_sum(u2.x + u2.y);
             if (lane == 0) red_s[par][warp] = part;
@@ -1329,25 +1402,20 @@ struct RowPlan {
 using RowKernelFn = void (*)(const RowArgs);
 
 template <typename T>
-RowKernelFn row_kernel_typed(int ept, int threads) {
-    if (threads == 1024) return ept == 16 ? row_sweep_kernel<T, 16, 1024> : row_sweep_kernel<T, 32, 1024>;
+RowKernelFn row_kernel_typed(int ept) {
     return ept == 16 ? row_sweep_kernel<T, 16, 512>
                      : (ept == 32 ? row_sweep_kernel<T, 32, 512> : row_sweep_kernel<T, 64, 512>);
 }
 
 RowKernelFn row_kernel_for(int dt, int ept, int threads) {
-    return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16>(ept, threads) : row_kernel_typed<__half>(ept, threads);
+    (void)threads;
+    return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16>(ept) : row_kernel_typed<__half>(ept);
 }
 
-// Threads per row-sweep CTA: 512 (measured faster than 1024 at n = 16384 and
-// 32768: 1024 threads halve the columns per thread, so the per-row reduction
-// and barrier cost more per element); FUGAL_ROW_THREADS=1024 selects the wider
-// CTA above 8192 columns.
-int row_threads_for(int64_t n_pad) {
-    const char* e = getenv("FUGAL_ROW_THREADS");
-    if (e != nullptr && atoi(e) == 1024 && n_pad > 8192) return 1024;
-    return 512;
-}
+// Threads per row-sweep CTA: 512.  (A 1024-thread CTA halves the columns per
+// thread; at n = 16384 and 32768 the extra per-row reduction and barrier cost
+// made it slower.)
+int row_threads_for(int64_t) { return 512; }
 
 fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool set_attributes) {
     rp = RowPlan{};
