@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     __shared__ uint64_t full[kMaxStages];
     __shared__ __align__(16) float red_s[2][kRowWarps];
     __shared__ __align__(16) float red_m[2][kRowWarps];
-    __shared__ __align__(16) float2 red_pair[2][kRowWarps];
+    __shared__ __align__(16) float red_grp[2][4][kRowWarps];
     __shared__ uint32_t tmem_slot;
 
     SolveState* st = p.st;
@@ -791,67 +791,74 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
 
     bool alive = true;
     int r = 0;
-    // Rows in pairs (one-segment rows, fast path): both rows' exponentials stay in
-    // registers, so the two rows share one barrier, one read of the per-warp sums
-    // and one pass over the TMEM accumulators.  A pair with a row outside the fast
-    // path's range hands the rest of the sweep to the single-row loop below,
-    // which restarts at that pair (its stages are still held).
+    // Rows in groups of RB = 64 / EPT (one-segment rows, fast path): the group's
+    // exponentials stay in registers, so its rows share one barrier, one read of
+    // the per-warp sums and one pass over the TMEM accumulators.  A group with a
+    // row outside the fast path's range hands the rest of the sweep to the
+    // single-row loop below, which restarts at that group (stages still held).
     if constexpr (NSEG == 1 && EPT <= 32) {
+        constexpr int RB = 64 / EPT;  // 2 or 4
         if (!exact_only) {
-            for (; r < nrows; r += 2) {
-                const int nr = min(2, nrows - r);
-                const int par = (r >> 1) & 1;
+            for (; r < nrows; r += RB) {
+                const int nr = min(RB, nrows - r);
+                const int par = (r / RB) & 1;
                 bool ok = true;
-                float2 ya[H], yb[H];
-                float2 sa = make_float2(0.f, 0.f), ta = sa, sb = sa, tb = sa;
-                row_fast(r, ya, sa, ta, ok);
-                if (nr == 2) {
-                    row_fast(r + 1, yb, sb, tb, ok);
-                } else {
+                float2 yg[RB][H];
+                float part[RB];
 #pragma unroll
-                    for (int h = 0; h < H; ++h) yb[h] = make_float2(0.f, 0.f);
+                for (int k = 0; k < RB; ++k) {
+                    float2 sa = make_float2(0.f, 0.f), ta = sa;
+                    if (k < nr) {
+                        row_fast(r + k, yg[k], sa, ta, ok);
+                    } else {
+#pragma unroll
+                        for (int h = 0; h < H; ++h) yg[k][h] = make_float2(0.f, 0.f);
+                    }
+                    const float2 ua = __fadd2_rn(sa, ta);
+                    part[k] = ua.x + ua.y;
                 }
-                const float2 ua = __fadd2_rn(sa, ta), ub = __fadd2_rn(sb, tb);
-                float pa = ua.x + ua.y, pb = ub.x + ub.y;
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) {
-                    pa += __shfl_xor_sync(0xffffffffu, pa, o);
-                    pb += __shfl_xor_sync(0xffffffffu, pb, o);
+#pragma unroll
+                    for (int k = 0; k < RB; ++k) part[k] += __shfl_xor_sync(0xffffffffu, part[k], o);
                 }
-                if (lane == 0) red_pair[par][warp] = make_float2(pa, pb);
+                if (lane == 0) {
+#pragma unroll
+                    for (int k = 0; k < RB; ++k) red_grp[par][k][warp] = part[k];
+                }
                 if (!__syncthreads_and(ok)) {
                     alive = false;
                     break;
                 }
-                float SA = 0.f, SB = 0.f;
+                float S[RB], wk[RB];
+                bool in_range = true;
 #pragma unroll
-                for (int w = 0; w < kRowWarps; ++w) {
-                    const float2 q = red_pair[par][w];
-                    SA += q.x;
-                    SB += q.y;
+                for (int k = 0; k < RB; ++k) {
+                    S[k] = 0.f;
+#pragma unroll
+                    for (int w = 0; w < kRowWarps; ++w) S[k] += red_grp[par][k][w];
+                    if (k < nr && !(S[k] > 1e-30f && S[k] < 1e30f)) in_range = false;
                 }
-                const bool in_range = SA > 1e-30f && SA < 1e30f && (nr < 2 || (SB > 1e-30f && SB < 1e30f));
                 if (!in_range) break;  // uniform
-                release(r);
-                if (nr == 2) release(r + 1);
-                const float wa = __frcp_rn(SA), wb = nr == 2 ? __frcp_rn(SB) : 0.f;
-                if (tid == 0) {
-                    p.a[row_begin + r] = -__log2f(SA) * kLn2;
-                    if (nr == 2) p.a[row_begin + r + 1] = -__log2f(SB) * kLn2;
-                }
-                const float2 wa2 = make_float2(wa, wa), wb2 = make_float2(wb, wb);
 #pragma unroll
-                for (int k = 0; k < EPT / 16; ++k) {
+                for (int k = 0; k < RB; ++k) {
+                    if (k < nr) release(r + k);
+                    wk[k] = k < nr ? __frcp_rn(S[k]) : 0.f;
+                    if (tid == 0 && k < nr) p.a[row_begin + r + k] = -__log2f(S[k]) * kLn2;
+                }
+#pragma unroll
+                for (int c = 0; c < EPT / 16; ++c) {
                     float acc[16];
-                    tmem_ld16(tcol + 16 * k, acc);
+                    tmem_ld16(tcol + 16 * c, acc);
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
-                        float2 a2 = __ffma2_rn(ya[8 * k + q], wa2, make_float2(acc[2 * q], acc[2 * q + 1]));
-                        a2 = __ffma2_rn(yb[8 * k + q], wb2, a2);
+                        float2 a2 = make_float2(acc[2 * q], acc[2 * q + 1]);
+#pragma unroll
+                        for (int k = 0; k < RB; ++k) a2 = __ffma2_rn(yg[k][8 * c + q], make_float2(wk[k], wk[k]), a2);
                         acc[2 * q] = a2.x;
                         acc[2 * q + 1] = a2.y;
                     }
-                    tmem_st16(tcol + 16 * k, acc);
+                    tmem_st16(tcol + 16 * c, acc);
                 }
             }
         }
