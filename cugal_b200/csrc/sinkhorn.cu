@@ -1063,32 +1063,36 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const float* part
 // online (max, sum) of exp(cost_ij + a_i).
 __global__ void __launch_bounds__(256) column_pass_kernel(const float* L, long long ld, int n, const float* a,
                                                           int rows_per_chunk, float2* part, long long n_pad) {
+    // Per column and row chunk: online (max, sum) of 2^((L_ij + a_i) log2 e), base-2 units,
+    // eight rows per step (their loads are all in flight before the exponentials).
     const int j0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int chunk = blockIdx.y;
     const int i0 = chunk * rows_per_chunk;
     const int i1 = min(n, i0 + rows_per_chunk);
     if (j0 >= n) return;
     const bool full4 = (j0 + 4 <= n) && ((ld & 3) == 0);
+    constexpr int RR = 8;
     float m[4], s[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         m[q] = -INFINITY;
         s[q] = 0.f;
     }
-    for (int i = i0; i < i1; i += 4) {
-        float x[4][4];
+    for (int i = i0; i < i1; i += RR) {
+        float x[RR][4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < RR; ++r) {
             const int row = i + r;
             if (row < i1) {
                 const float ai = a[row];
                 const float* src = L + static_cast<size_t>(row) * ld + j0;
                 if (full4) {
                     const float4 v = *reinterpret_cast<const float4*>(src);
-                    x[r][0] = v.x + ai; x[r][1] = v.y + ai; x[r][2] = v.z + ai; x[r][3] = v.w + ai;
+                    x[r][0] = (v.x + ai) * kLog2e; x[r][1] = (v.y + ai) * kLog2e;
+                    x[r][2] = (v.z + ai) * kLog2e; x[r][3] = (v.w + ai) * kLog2e;
                 } else {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) x[r][q] = (j0 + q < n) ? src[q] + ai : -INFINITY;
+                    for (int q = 0; q < 4; ++q) x[r][q] = (j0 + q < n) ? (src[q] + ai) * kLog2e : -INFINITY;
                 }
             } else {
 #pragma unroll
@@ -1097,11 +1101,13 @@ __global__ void __launch_bounds__(256) column_pass_kernel(const float* L, long l
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const float mn = fmaxf(fmaxf(m[q], fmaxf(x[0][q], x[1][q])), fmaxf(x[2][q], x[3][q]));
-            if (mn == -INFINITY) continue;
-            float acc = (m[q] == -INFINITY) ? 0.f : s[q] * expf(m[q] - mn);
+            float mn = m[q];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) acc += expf(x[r][q] - mn);
+            for (int r = 0; r < RR; ++r) mn = fmaxf(mn, x[r][q]);
+            if (mn == -INFINITY) continue;
+            float acc = (m[q] == -INFINITY) ? 0.f : s[q] * ex2(m[q] - mn);
+#pragma unroll
+            for (int r = 0; r < RR; ++r) acc += ex2(x[r][q] - mn);
             m[q] = mn;
             s[q] = acc;
         }
@@ -1153,9 +1159,9 @@ __global__ void column_merge_kernel(const float2* part, int nchunks, long long n
         if (M != -INFINITY)
             for (int c = 0; c < nchunks; ++c) {
                 const float2 ps = part[static_cast<size_t>(c) * n_pad + j];
-                if (ps.x != -INFINITY) S += ps.y * expf(ps.x - M);
+                if (ps.x != -INFINITY) S += ps.y * ex2(ps.x - M);
             }
-        b_buf[n_pad + j] = -(M + logf(S));  // slot of sweep -1
+        b_buf[n_pad + j] = -(M + log2f(S)) * kLn2;  // slot of sweep -1 (partials are in base-2 units)
         logcs[j] = 0.f;
     }
 }
