@@ -213,6 +213,21 @@ def test_row_sweep_matches_cluster_sweep_and_fp32(n, monkeypatch):
     np.testing.assert_allclose(P_r.sum(axis=1), 1.0, atol=1e-3)
 
 
+@pytest.mark.parametrize("warmup", [0, 1])
+def test_reduced_precision_without_fp32_warmup(warmup):
+    """The absorb sweep may be the first sweep of a solve (no FP32 warm-up)."""
+    n = 3000
+    rng = np.random.default_rng(5)
+    C = (rng.random((n, n)) * 4).astype(np.float32).astype(np.float64)
+    zero = np.zeros(n)
+    reg = 0.05
+    ref = O.sinkhorn_log_solve(C, zero, zero, reg, 40, 0.0, 10)
+    u, v, prof = _solve_gpu(C, zero, zero, reg, 40, 0.0, 10, stream_dtype=torch.bfloat16, polish=1, warmup=warmup,
+                            every=20)
+    assert prof.iteration_count == 40
+    np.testing.assert_allclose(_plan(C, u, v, reg), _plan(C, ref.u, ref.v, reg), atol=1e-2)
+
+
 def test_row_sweep_momentum_matches_oracle():
     n = 3000
     rng = np.random.default_rng(21)
