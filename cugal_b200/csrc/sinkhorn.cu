@@ -19,13 +19,18 @@
 // momentum change at an evaluation point affects v_{t+1} as in the reference).
 // Only the first column update of a solve is a separate max-stabilised pass.
 //
-// Row layout: each cluster of C CTAs owns a contiguous block of rows; CTA k of
-// the cluster owns column slice k.  Row slices stream HBM -> shared memory with
-// 1-D bulk copies (cp.async.bulk + mbarrier, several stages in flight); the
-// per-row (max, sum) partials of the C CTAs are exchanged through distributed
-// shared memory (remote stores + remote mbarrier arrives, double-buffered).
-// Every thread keeps its 16 columns' running column sums in registers for the
-// whole sweep, so the only global writes are one partial row per cluster.
+// Two sweep kernels share this structure.
+//   sweep_kernel (FP32 sweeps, the absorb sweep, and 16-bit sweeps wider than
+//   32768 columns): each cluster of C CTAs owns a contiguous block of rows; CTA
+//   k of the cluster owns column slice k.  Row slices stream HBM -> shared
+//   memory with 1-D bulk copies (cp.async.bulk + mbarrier, several stages in
+//   flight); the per-row (max, sum) partials of the C CTAs are exchanged through
+//   distributed shared memory (remote stores + remote mbarrier arrives,
+//   double-buffered).  Every thread keeps its 16 or 32 columns' running column
+//   sums in registers, so the only global writes are one partial row per cluster.
+//   row_sweep_kernel (16-bit sweeps up to 32768 columns): one 512-thread CTA per
+//   SM owns whole rows, the row normaliser is a CTA barrier, the column sums
+//   live in tensor memory (TMEM); see its own comment below.
 //
 // Precision: the cost arrives "absorbed" (cost32 = K + U_i + V_j with the
 // previous solves' duals U, V folded in), so its entries are ~log P and the
