@@ -63,6 +63,7 @@ def parse_args(argv=None):
                     help="differentiation workload instead: STEPS gradient steps on mu through the Sinkhorn adjoint")
     ap.add_argument("--fp32-warmup-sweeps", type=int, default=None, help="override Config.fp32_warmup_sweeps")
     ap.add_argument("--reabsorb-every", type=int, default=None, help="override Config.reabsorb_every")
+    ap.add_argument("--line-search", action="store_true", help="Config.line_search: exact Frank-Wolfe steps")
     return ap.parse_args(argv)
 
 
@@ -296,6 +297,8 @@ def run_ours(args):
         over["fp32_warmup_sweeps"] = args.fp32_warmup_sweeps
     if args.reabsorb_every is not None:
         over["reabsorb_every"] = args.reabsorb_every
+    if args.line_search:
+        over["line_search"] = True
     config = config_for(w, **over)
     n = src.number_of_nodes()
     A = Adjacency.from_graph(src, config.device)
@@ -396,7 +399,7 @@ def run_ours(args):
                        "fw_steps": config.iter_count * config.frank_wolfe_iter_count,
                        "sinkhorn_iterations": config.sinkhorn_iterations, "reg": config.sinkhorn_regularization,
                        "fp32_warmup_sweeps": config.fp32_warmup_sweeps, "reabsorb_every": config.reabsorb_every,
-                       "polish_sweeps": config.polish_sweeps,
+                       "polish_sweeps": config.polish_sweeps, "line_search": config.line_search,
                        "lap": config.hungarian_method.value, "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (cost copy n*ld*2 bytes)"},
             "node_accuracy": accuracy, "e2e_node_accuracy": e2e_acc,

@@ -92,6 +92,9 @@ SIGNATURES = {
     "fugal_sinkhorn_plan_info": (_INT, [_I64, _INT, _P]),
     "fugal_sinkhorn_solve": (_INT, [POINTER(SolveParams), _P, _SZ, _P]),
     "fugal_fw_update": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _P]),
+    "fugal_fw_direction": (_INT, [_I64, _P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _P, _I64, _P, _INT,
+                                  _P]),
+    "fugal_fw_line_search_update": (_INT, [_I64, _P, _I64, _P, _I64, _P, _I64, _D, _P, _P, _P, _P]),
     "fugal_timing_enable": (None, [_INT]),
     "fugal_timing_reset": (None, []),
     "fugal_timing_query": (_INT, [_INT, POINTER(c_int64), POINTER(c_double)]),

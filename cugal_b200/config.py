@@ -98,6 +98,12 @@ class Config:
     lap_candidates: int = 8
     """Per-row candidate columns kept by the greedy rounding kernels."""
 
+    line_search: bool = False
+    """Frank-Wolfe step by exact line search instead of ``2 / (2 + it)``: the
+    objective -<P, A P B> + <D, P> + lambda <P, 1 - P> is quadratic along the
+    direction q - P, so the step is the minimiser of that parabola on [0, 1],
+    computed on the device (one more pair of SpMM kernels per step)."""
+
     def convert_tensor(self, input: torch.Tensor) -> torch.Tensor:
         """Convert tensor to the configured dtype and device."""
         return input.to(dtype=self.dtype, device=self.device)

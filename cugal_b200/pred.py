@@ -92,6 +92,14 @@ class FrankWolfeEngine:
             self.solver = SinkhornSolver(n, self.config, dev)
         self.records = torch.empty((max(1, self.max_solves), N.RECORD_BYTES), dtype=torch.uint8, device=dev)
         self.solves = 0
+        self.updates = 0
+        self._fixed_alphas: list[float] = []
+        if self.config.line_search:
+            # direction q - P (padding columns stay zero: the SpMM reads whole rows),
+            # the three FP64 sums and the step of every update
+            self.dir_buf = torch.zeros((n, self.ld), dtype=torch.float32, device=dev)
+            self.ls_sums = torch.zeros(3, dtype=torch.float64, device=dev)
+            self.alphas = torch.zeros(max(1, self.max_solves), dtype=torch.float64, device=dev)
         if isinstance(self.features, Features):
             self.fs = self.features.source.float().contiguous()
             self.ft = self.features.target.float().contiguous()
@@ -134,7 +142,14 @@ class FrankWolfeEngine:
         self.solves += 1
         return k
 
-    def update(self, alpha: float) -> torch.Tensor:
+    def update(self, alpha: float, lam: float = 0.0) -> torch.Tensor:
+        """P += alpha (q - P) and the duality gap; with ``config.line_search`` the
+        step is the exact line-search minimiser (``alpha`` unused, ``lam`` the
+        gradient's lambda)."""
+        self.updates += 1
+        if self.config.line_search:
+            return self._line_search_update(lam)
+        self._fixed_alphas.append(float(alpha))
         if self.standard:
             N.call("fugal_fw_update_standard", self.n, self.P_buf.data_ptr(), self.ld, self.K_buf.data_ptr(), self.ld,
                    self.u.data_ptr(), self.v.data_ptr(), self.cost32.data_ptr(), self.ld, float(alpha),
@@ -144,6 +159,39 @@ class FrankWolfeEngine:
                self.u.data_ptr(), self.v.data_ptr(), self.U.data_ptr(), self.V.data_ptr(), float(alpha),
                float(self.config.sinkhorn_regularization), self.gap.data_ptr(), 1, N.stream_handle(self.device))
         return self.gap
+
+    def _line_search_update(self, lam: float) -> torch.Tensor:
+        k = self.updates - 1
+        if k >= self.alphas.numel():
+            self.alphas = torch.cat([self.alphas, torch.zeros_like(self.alphas)])
+        stream = N.stream_handle(self.device)
+        d = self.dir_buf
+        if self.standard:
+            N.call("fugal_fw_direction", self.n, self.P_buf.data_ptr(), self.ld, self.cost32.data_ptr(), self.ld,
+                   self.K_buf.data_ptr(), self.ld, self.u.data_ptr(), self.v.data_ptr(), None, None,
+                   float(self.config.sinkhorn_regularization), d.data_ptr(), self.ld, self.ls_sums.data_ptr(), 0,
+                   stream)
+        else:
+            N.call("fugal_fw_direction", self.n, self.P_buf.data_ptr(), self.ld, self.cost32.data_ptr(), self.ld,
+                   None, 0, self.u.data_ptr(), self.v.data_ptr(), self.U.data_ptr(), self.V.data_ptr(),
+                   float(self.config.sinkhorn_regularization), d.data_ptr(), self.ld, self.ls_sums.data_ptr(), 1,
+                   stream)
+        # W = -2 A d B into cost32, which the next gradient rewrites
+        W = self.cost32
+        N.call("fugal_fw_gradient", self.n, self.A.row_pointers.data_ptr(), self.A.col_indices.data_ptr(),
+               self.B.row_pointers.data_ptr(), self.B.col_indices.data_ptr(), d.data_ptr(), self.ld,
+               None, None, None, 0, 0.0, 1.0, 1.0, None, None, W.data_ptr(), self.ld,
+               self.grad_ws.data_ptr(), self.grad_ws.numel(), stream)
+        N.call("fugal_fw_line_search_update", self.n, self.P_buf.data_ptr(), self.ld, d.data_ptr(), self.ld,
+               W.data_ptr(), self.ld, float(lam) * self.lambda_scale, self.ls_sums.data_ptr(),
+               self.alphas[k:].data_ptr(), self.gap.data_ptr(), stream)
+        return self.gap
+
+    def step_lengths(self) -> np.ndarray:
+        """Steps of the updates so far (the line-search minimisers, or 2/(2+it))."""
+        if self.config.line_search:
+            return self.alphas[:self.updates].cpu().numpy()
+        return np.asarray(self._fixed_alphas)
 
     def sinkhorn_profiles(self) -> list[SinkhornProfile]:
         raw = self.records[:self.solves].cpu()
@@ -231,13 +279,14 @@ def find_quasi_permutation_matrix(A: Adjacency, B: Adjacency, features: Features
             profile.log_time(start_time, Phase.SINKHORN)
 
             alpha = 2.0 / float(2.0 + it)
-            gap = engine.update(alpha)
+            gap = engine.update(alpha, lam)
             profile.frank_wolfe_iterations += 1
             if config.frank_wolfe_threshold is not None and abs(float(gap.item())) < config.frank_wolfe_threshold:
                 break
     for (s, e), sp in zip(solve_times, engine.sinkhorn_profiles()):
         sp.time = e.elapsed_seconds(s)
         profile.sinkhorn_profiles.append(sp)
+    profile._steps.extend(float(a) for a in engine.step_lengths())
     if config.safe_mode:
         assert engine.P.isfinite().all(), "quasi_permutation tensor has NaN values"
     return engine.P

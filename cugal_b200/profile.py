@@ -74,6 +74,13 @@ class Profile:
     sparsity: float = 0.0
     # Event pairs not yet folded into phase_times (not part of to_dict()).
     _pending: list = field(default_factory=list, repr=False, compare=False)
+    # Frank-Wolfe step of every update, 2/(2+it) or the line-search minimiser
+    # (not part of to_dict(): the reference's Profile has no such field).
+    _steps: list = field(default_factory=list, repr=False, compare=False)
+
+    @property
+    def frank_wolfe_steps(self) -> list[float]:
+        return list(self._steps)
 
     def log_time(self, start_time: TimeStamp, phase: Phase):
         now = TimeStamp(start_time.device)

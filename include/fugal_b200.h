@@ -327,6 +327,34 @@ fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const float* cost
                              const float* u, const float* v, double* U, double* V, double alpha,
                              double regularization, double* gap, int commit, fugal_stream_t stream);
 
+/* Exact line search, opt-in (Config.line_search).  No counterpart in the
+ * reference, which steps with alpha = 2/(2+it) (cugal/pred.py:133-141).  On the
+ * objective f(P) = -<P, A P B> + <D, P> + lam' <P, 1 - P>, whose gradient is the
+ * one fugal_fw_gradient builds, f(P + a d) - f(P) = a g + a^2 Q exactly, with
+ * d = q - P, g = <G, d>, Q = -<d, A d B> - lam' <d, d>.  Three calls:
+ *
+ * fugal_fw_direction: dir = q - P (FP32, columns [0, n) written) and, in FP64,
+ * sums[0] = g, sums[1] = <d, d>, sums[2] = 0 (sums: 3 DEVICE doubles).  Log form
+ * (K == NULL): q = exp(cost32 + u_i + v_j), G = -reg (cost32 - U_i - V_j), and
+ * commit != 0 folds the duals as fugal_fw_update does.  Scaling form: q =
+ * (K_ij v_j) u_i, G = cost32 (the plain gradient), U = V = NULL, commit = 0.
+ *
+ * fugal_fw_gradient with P := dir, no features or distance, lambda = 0,
+ * out_scale = 1, U = V = NULL gives W = -2 A d B.
+ *
+ * fugal_fw_line_search_update: sums[2] = <d, W>, then a = argmin over [0, 1] of
+ * a g + a^2 Q with Q = sums[2]/2 - lambda_eff sums[1] (Q > 0: -g/2Q clipped;
+ * else 1 if g + Q < 0, else 0), P += a dir, *alpha = a and *gap = g (DEVICE
+ * doubles; either may be NULL).  lambda_eff = lambda * lambda_scale of the
+ * gradient.  Nothing is read back to the host. */
+fugal_status fugal_fw_direction(int64_t n, const float* P, int64_t ldp, const float* cost32, int64_t ld32,
+                                const float* K, int64_t ldk, const float* u, const float* v, double* U, double* V,
+                                double regularization, float* dir, int64_t ldd, double* sums, int commit,
+                                fugal_stream_t stream);
+fugal_status fugal_fw_line_search_update(int64_t n, float* P, int64_t ldp, const float* dir, int64_t ldd,
+                                         const float* W, int64_t ldw, double lambda_eff, double* sums,
+                                         double* alpha, double* gap, fugal_stream_t stream);
+
 /* ======================= instrumentation ================================== */
 /* When enabled, every kernel of the families above is bracketed by CUDA events
  * on its launch stream; totals are accumulated when a solve polls its progress

@@ -346,6 +346,35 @@ def duality_gap(G: np.ndarray, diff: np.ndarray, alpha: float) -> float:
     return abs(float(np.sum(G * (diff / alpha))))
 
 
+def apb(A, B, X: np.ndarray) -> np.ndarray:
+    """A X B for sparse or dense symmetric A, B (the product ``sparse_gradient`` forms)."""
+    AX = np.asarray(A @ X)
+    return np.asarray(B.T @ AX.T).T
+
+
+def fw_objective(A, B, P: np.ndarray, D: np.ndarray, lam_eff: float) -> float:
+    """-<P, A P B> + <D, P> + lam_eff <P, 1 - P>: the objective whose gradient is
+    ``sparse_gradient`` (``cugal/pred.py:54-74``) for symmetric A, B."""
+    return float(-np.sum(P * apb(A, B, P)) + np.sum(D * P) + lam_eff * np.sum(P * (1.0 - P)))
+
+
+def line_search_alpha(g: float, Q: float) -> float:
+    """argmin over a in [0, 1] of a g + a^2 Q."""
+    if Q > 0:
+        return min(1.0, max(0.0, -g / (2.0 * Q)))
+    return 1.0 if g + Q < 0 else 0.0
+
+
+def line_search_step(A, B, P: np.ndarray, G: np.ndarray, q: np.ndarray, lam_eff: float):
+    """Exact line search along d = q - P (opt-in; the reference steps with
+    2/(2+it), ``cugal/pred.py:133``): f(P + a d) - f(P) = a g + a^2 Q with
+    g = <G, d>, Q = -<d, A d B> - lam_eff <d, d>.  Returns (a, g, Q)."""
+    d = q - P
+    g = float(np.sum(G * d))
+    Q = -float(np.sum(d * apb(A, B, d))) - lam_eff * float(np.sum(d * d))
+    return line_search_alpha(g, Q), g, Q
+
+
 # --------------------------------------------------------------------------
 # Rounding                          (cugal/greedy_lap.py:7-85, pred.py:151-193)
 # --------------------------------------------------------------------------
@@ -448,6 +477,7 @@ class OracleParams:
     hungarian_method: str = "SCIPY"
     mutating_marginal: bool = False
     double_lambda: bool = True   # only read by the dense gradient
+    line_search: bool = False    # exact line search instead of 2/(2+it) (no reference counterpart)
 
 
 @dataclass
@@ -455,6 +485,7 @@ class FWTrace:
     sinkhorn_iterations: list = field(default_factory=list)
     sinkhorn_errors: list = field(default_factory=list)
     gaps: list = field(default_factory=list)
+    alphas: list = field(default_factory=list)
     frank_wolfe_iterations: int = 0
 
 
@@ -484,13 +515,24 @@ def find_quasi_permutation_matrix(A_csr, B_csr, D: np.ndarray, p: OracleParams,
                                               p.sinkhorn_threshold, p.sinkhorn_eval_freq,
                                               p.sinkhorn_momentum_start)
             u, v = res.u, res.v
-            alpha = 2.0 / float(2.0 + it)
-            diff = update_quasi_permutation(P, res.K, u, v, alpha, p.sinkhorn_method == "LOG")
-            gap = duality_gap(G, diff, alpha)
+            if p.line_search:
+                if p.sinkhorn_method == "LOG":
+                    q = np.exp(res.K + u[:, None] + v[None, :])
+                else:
+                    q = res.K * v[None, :] * u[:, None]
+                dense_twice = not p.use_sparse_adjacency and p.double_lambda
+                alpha, g, _ = line_search_step(A, B, P, G, q, lam * (2.0 if dense_twice else 1.0))
+                P += alpha * (q - P)
+                gap = abs(g)
+            else:
+                alpha = 2.0 / float(2.0 + it)
+                diff = update_quasi_permutation(P, res.K, u, v, alpha, p.sinkhorn_method == "LOG")
+                gap = duality_gap(G, diff, alpha)
             if trace is not None:
                 trace.sinkhorn_iterations.append(res.iteration_count)
                 trace.sinkhorn_errors.append(res.errors)
                 trace.gaps.append(gap)
+                trace.alphas.append(alpha)
                 trace.frank_wolfe_iterations += 1
             if p.frank_wolfe_threshold is not None and gap < p.frank_wolfe_threshold:
                 break
