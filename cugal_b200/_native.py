@@ -38,6 +38,7 @@ class SolveParams(ctypes.Structure):
         ("stream_dtype", c_int), ("max_iterations", c_int), ("threshold", c_double), ("eval_freq", c_int),
         ("momentum_start", c_int), ("fp32_warmup_sweeps", c_int), ("reabsorb_every", c_int),
         ("polish_sweeps", c_int), ("u_out", c_void_p), ("v_out", c_void_p), ("record", c_void_p),
+        ("column_partials", c_void_p), ("column_partial_chunks", ctypes.c_int32), ("column_partial_ld", c_int64),
     ]
 
 
@@ -91,6 +92,9 @@ SIGNATURES = {
     "fugal_sinkhorn_workspace_size": (_INT, [_I64, _INT, POINTER(c_size_t)]),
     "fugal_sinkhorn_plan_info": (_INT, [_I64, _INT, _P]),
     "fugal_sinkhorn_solve": (_INT, [POINTER(SolveParams), _P, _SZ, _P]),
+    "fugal_gradient_column_chunks": (_INT, [_I64, POINTER(ctypes.c_int32)]),
+    "fugal_fw_gradient_column_stats": (_INT, [_I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _I64, _D, _D, _D, _P, _P,
+                                              _P, _I64, _P, _SZ, _P, _I64, _P]),
     "fugal_fw_update": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _P]),
     "fugal_fw_direction": (_INT, [_I64, _P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _P, _I64, _P, _INT,
                                   _P]),

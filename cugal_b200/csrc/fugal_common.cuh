@@ -90,6 +90,16 @@ FUGAL_DEVICE double block_sum(double v, double* scratch) {
 // error a few ulp, the same primitive the reference kernels use).
 FUGAL_DEVICE float fast_exp(float x) { return __expf(x); }
 
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kLn2 = 0.6931471805599453f;
+
+// 2^x on the MUFU unit (PTX ex2.approx.ftz.f32).
+FUGAL_DEVICE float ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // ------------------------------------------------------- element conversion
 template <typename T> struct Vec;  // one 16-byte chunk of T as fp32
 

@@ -148,18 +148,9 @@ struct SweepArgs {
 
 constexpr int kBarBytes = 128;
 
-constexpr float kLog2e = 1.4426950408889634f;
-constexpr float kLn2 = 0.6931471805599453f;
 // Largest |column correction| (nats) after which the next sweep uses the exact
 // (max-stabilised) row reduction instead of the previous row normaliser.
 constexpr float kFastPathLimit = 30.0f;
-
-// 2^x on the MUFU unit (PTX ex2.approx.ftz.f32).
-FUGAL_DEVICE float ex2(float x) {
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
 
 // Sum (or max) of one value per lane, the same in every lane.  The sum is lane
 // 0's butterfly result broadcast: every warp that reduces the same inputs then
@@ -1129,11 +1120,16 @@ struct InitArgs {
     double threshold;
 };
 
-// Merge the column-pass partials into v_0 = -LSE_i(cost + a) (momentum is 1 at
-// iteration 0), stored as the "previous sweep" b, with a zero pending
-// correction; block 0 also resets the solve state.
-__global__ void column_merge_kernel(const float2* part, int nchunks, long long n_pad, int n, float* b_buf,
-                                    float* logcs, SolveState* st, InitArgs ia) {
+// Merge base-2 column partials (max, sum) into v_0 = -LSE_i(cost + a) (momentum
+// is 1 at iteration 0), stored as the "previous sweep" b, with a zero pending
+// correction; block 0 also resets the solve state.  A block takes 32 columns;
+// its 8 warps split the chunks (each a two-pass max-then-sum), then warp 0
+// combines the 8 pairs.  Grid: ceil(n / 32) blocks of 256 threads.
+constexpr int kMergeLanes = 8;
+__global__ void __launch_bounds__(256) column_merge_kernel(const float2* part, int nchunks, long long part_ld,
+                                                           long long n_pad, int n, float* b_buf, float* logcs,
+                                                           SolveState* st, InitArgs ia) {
+    __shared__ float2 red[kMergeLanes][32];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st->it = 0;
         st->done = 0;
@@ -1157,16 +1153,32 @@ __global__ void column_merge_kernel(const float2* part, int nchunks, long long n
         st->main_last_err = 0.0;
         st->polish_err = 0.0;
     }
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        float M = -INFINITY;
-        for (int c = 0; c < nchunks; ++c) M = fmaxf(M, part[static_cast<size_t>(c) * n_pad + j].x);
-        float S = 0.f;
+    const int lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
+    const int j = blockIdx.x * 32 + lane;
+    float M = -INFINITY, S = 0.f;
+    if (j < n) {
+        for (int c = grp; c < nchunks; c += kMergeLanes) M = fmaxf(M, part[static_cast<size_t>(c) * part_ld + j].x);
         if (M != -INFINITY)
-            for (int c = 0; c < nchunks; ++c) {
-                const float2 ps = part[static_cast<size_t>(c) * n_pad + j];
+            for (int c = grp; c < nchunks; c += kMergeLanes) {
+                const float2 ps = part[static_cast<size_t>(c) * part_ld + j];
                 if (ps.x != -INFINITY) S += ps.y * ex2(ps.x - M);
             }
-        b_buf[n_pad + j] = -(M + log2f(S)) * kLn2;  // slot of sweep -1 (partials are in base-2 units)
+    }
+    red[grp][lane] = make_float2(M, S);
+    __syncthreads();
+    if (grp == 0 && j < n) {
+        float Mt = -INFINITY;
+#pragma unroll
+        for (int g = 0; g < kMergeLanes; ++g) Mt = fmaxf(Mt, red[g][lane].x);
+        float St = 0.f;
+        if (Mt != -INFINITY) {
+#pragma unroll
+            for (int g = 0; g < kMergeLanes; ++g) {
+                const float2 ps = red[g][lane];
+                if (ps.x != -INFINITY) St += ps.y * ex2(ps.x - Mt);
+            }
+        }
+        b_buf[n_pad + j] = -(Mt + log2f(St)) * kLn2;  // slot of sweep -1 (partials are in base-2 units)
         logcs[j] = 0.f;
     }
 }
@@ -1203,7 +1215,10 @@ __global__ void polish_begin_kernel(SolveState* st, float* a, float* b_buf, long
         st->max_it = fin + 1 + f.polish;
         st->check = 0;
         st->omega = 1.0;
-        st->exact_next = 1;
+        // the polish sweep's column step is zero (logcs cleared above), so the
+        // previous row normaliser is a safe reference: fast path, with the
+        // per-row fallback to the exact path when a row sum leaves its range
+        st->exact_next = 0;
     }
 }
 
@@ -1602,6 +1617,10 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_solve: cost16 needs ld >= n, ld %% 8 == 0, 16-byte base");
     if (use16 && (p.fp32_warmup_sweeps < 0 || p.reabsorb_every <= 0 || p.polish_sweeps < 0))
         return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: bad reduced-precision schedule");
+    if (p.column_partials != nullptr &&
+        (p.column_partial_chunks <= 0 || p.column_partial_ld < n ||
+         (reinterpret_cast<uintptr_t>(p.column_partials) & 7u) != 0))
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: column partials need chunks > 0, ld >= n, 8-byte base");
 
     const int prow = partial_rows_bound(n);
     Workspace w = layout(n, static_cast<char*>(workspace), prow);
@@ -1624,10 +1643,17 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
     FrameArgs frame{use16 ? 1 : 0, use16 ? p.fp32_warmup_sweeps : 0, use16 ? p.reabsorb_every : 1,
                     use16 ? p.polish_sweeps : 0};
 
-    // ---- iteration 0, column update: v_0 = -LSE_i(cost32_ij + a_i), a = 0
+    // ---- iteration 0, column update: v_0 = -LSE_i(cost32_ij + a_i), a = 0, from
+    //      the caller's column partials (written with the cost) or a pass over cost32
     FUGAL_TRY(cuda_check(cudaMemsetAsync(w.a, 0, w.n_pad * 4, stream), "sinkhorn: clear row duals"));
-    const int chunks = colpass_chunks(n);
-    {
+    const float2* part = reinterpret_cast<const float2*>(w.partials);
+    int chunks = colpass_chunks(n);
+    long long part_ld = w.n_pad;
+    if (p.column_partials != nullptr) {
+        part = reinterpret_cast<const float2*>(p.column_partials);
+        chunks = p.column_partial_chunks;
+        part_ld = p.column_partial_ld;
+    } else {
         const int rows_per_chunk = static_cast<int>((n + chunks - 1) / chunks);
         dim3 grid(static_cast<unsigned>((n + kColThreads * 4 - 1) / (kColThreads * 4)), chunks);
         LaunchScope scope(FUGAL_KERNEL_COLUMN_PASS, stream);
@@ -1640,9 +1666,8 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
     {
         InitArgs ia{p.max_iterations, p.eval_freq, p.momentum_start < 0 ? -1 : p.momentum_start, p.threshold};
         LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
-        column_merge_kernel<<<fin_blocks, 256, 0, stream>>>(reinterpret_cast<const float2*>(w.partials), chunks,
-                                                           w.n_pad, static_cast<int>(n), w.b_buf, w.logcs, w.st,
-                                                           ia);
+        column_merge_kernel<<<static_cast<unsigned>((n + 31) / 32), 256, 0, stream>>>(
+            part, chunks, part_ld, w.n_pad, static_cast<int>(n), w.b_buf, w.logcs, w.st, ia);
         FUGAL_TRY(launch_check("sinkhorn: column merge"));
     }
 

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 
 #include "fugal_common.cuh"
 #include "fugal_host.h"
@@ -149,17 +150,26 @@ struct EpilogueArgs {
     const double* V;
     float* out;
     long long ldo;
+    float2* colpart;  // COLSTATS: [n / 128 panels][ldc] base-2 (max, sum) of out's columns
+    long long ldc;
 };
 
 // Y = B Tt = (APB)^T over the tile (rows j0.., cols i0..), then the gradient
-// epilogue in (i, j) orientation.
+// epilogue in (i, j) orientation.  COLSTATS: the CTA also reduces, for each of
+// its 32 output columns j, the 128 values it wrote over rows i0 .. i0+127 to a
+// base-2 (max, sum) pair, x = out log2 e: M = max x, S = sum 2^(x - M), stored
+// at colpart[blockIdx.y][j] (the first column update of the Sinkhorn solve
+// merges them instead of reading the cost again).
+template <bool COLSTATS>
 __global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __restrict__ rp,
                                                                 const int* __restrict__ col,
                                                                 const float* __restrict__ Tt, long long ldt, int n,
                                                                 const EpilogueArgs ep) {
+    constexpr int kWarps = kSpmmThreads / 32;
     __shared__ float tile[kTileRows][kTileCols + 1];
     __shared__ float4 fi[kTileCols];
     __shared__ float4 fj[kTileRows];
+    __shared__ float2 cst[COLSTATS ? kWarps : 1][kTileRows];
     const int j0 = blockIdx.x * kTileRows;   // gathered rows: target nodes j
     const int i0 = blockIdx.y * kTileCols;   // lanes: source nodes i
     const bool has_f = ep.fs != nullptr;
@@ -173,13 +183,14 @@ __global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __res
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = j0 + lane;
-    if (j >= n) return;
-    const double vj = ep.V ? ep.V[j] : 0.0;
+    if (!COLSTATS && j >= n) return;
+    const double vj = (ep.V && j < n) ? ep.V[j] : 0.0;
     const float4 f2 = has_f ? fj[lane] : make_float4(0, 0, 0, 0);
     const float lam = static_cast<float>(ep.lam);
-    for (int ii = warp; ii < kTileCols; ii += kSpmmThreads / 32) {
+    float xmax = -INFINITY;
+    for (int ii = warp; ii < kTileCols; ii += kWarps) {
         const int i = i0 + ii;
-        if (i >= n) break;
+        if (i >= n || j >= n) break;
         // The gradient itself in FP32, as the reference computes it (SpMM, distance,
         // regularize: cugal/pred.py:54-74, distance.cu:11-53, regularize.cu:10-39) ...
         const float apb = tile[lane][ii];
@@ -196,7 +207,37 @@ __global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __res
         // ... and its combination with the accumulated duals in FP64: the terms are
         // O(1/reg) and cancel to O(1), which FP32 would not resolve.
         const double ui = ep.U ? ep.U[i] : 0.0;
-        ep.out[static_cast<size_t>(i) * ep.ldo + j] = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + vj));
+        const float o = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + vj));
+        ep.out[static_cast<size_t>(i) * ep.ldo + j] = o;
+        if constexpr (COLSTATS) {
+            // the tile entry this thread just consumed keeps x = out log2 e for the sum below
+            const float x = o * kLog2e;
+            tile[lane][ii] = x;
+            xmax = fmaxf(xmax, x);
+        }
+    }
+    if constexpr (COLSTATS) {
+        // second pass over the same tile entries (this thread's own, no barrier needed)
+        float sum = 0.f;
+        if (xmax != -INFINITY) {
+            for (int ii = warp; ii < kTileCols && i0 + ii < n; ii += kWarps) sum += ex2(tile[lane][ii] - xmax);
+        }
+        cst[warp][lane] = make_float2(xmax, sum);
+        __syncthreads();
+        if (warp == 0 && j < n) {
+            float M = -INFINITY;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) M = fmaxf(M, cst[w][lane].x);
+            float S = 0.f;
+            if (M != -INFINITY) {
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w) {
+                    const float2 ps = cst[w][lane];
+                    if (ps.x != -INFINITY) S += ps.y * ex2(ps.x - M);
+                }
+            }
+            ep.colpart[static_cast<size_t>(blockIdx.y) * ep.ldc + j] = make_float2(M, S);
+        }
     }
 }
 
@@ -259,14 +300,14 @@ extern "C" fugal_status fugal_gradient_workspace_size(int64_t n, size_t* bytes) 
     return FUGAL_OK;
 }
 
-extern "C" fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices,
-                                          const int32_t* b_row_pointers, const int32_t* b_col_indices,
-                                          const float* P, int64_t ldp, const float* source_features,
-                                          const float* target_features, const float* D, int64_t ldd,
-                                          double lambda, double lambda_scale, double out_scale, const double* U,
-                                          const double* V, float* out, int64_t ldo, void* workspace,
-                                          size_t workspace_bytes, fugal_stream_t stream_) {
-    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+namespace {
+
+fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices,
+                         const int32_t* b_row_pointers, const int32_t* b_col_indices, const float* P, int64_t ldp,
+                         const float* source_features, const float* target_features, const float* D, int64_t ldd,
+                         double lambda, double lambda_scale, double out_scale, const double* U, const double* V,
+                         float* out, int64_t ldo, void* workspace, size_t workspace_bytes, float* column_partials,
+                         int64_t ldc, cudaStream_t stream) {
     FUGAL_TRY(check_csr(a_row_pointers, a_col_indices, n, "fugal_fw_gradient(A)"));
     FUGAL_TRY(check_csr(b_row_pointers, b_col_indices, n, "fugal_fw_gradient(B)"));
     if (P == nullptr || out == nullptr || workspace == nullptr)
@@ -281,6 +322,8 @@ extern "C" fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointe
         return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: P needs ld >= n, ld %% 4 == 0, 16-byte base");
     if (source_features && (!aligned16(source_features) || !aligned16(target_features)))
         return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: feature rows must be 16-byte aligned");
+    if (column_partials != nullptr && (ldc < n || (reinterpret_cast<uintptr_t>(column_partials) & 7u) != 0))
+        return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient_column_stats: partials need ldc >= n and 8-byte alignment");
     size_t need = 0;
     FUGAL_TRY(fugal_gradient_workspace_size(n, &need));
     if (workspace_bytes < need || !aligned16(workspace))
@@ -295,13 +338,51 @@ extern "C" fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointe
                                                               static_cast<int>(n), Tt, ldt, 1, 1.f);
         FUGAL_TRY(launch_check("fugal_fw_gradient: A P"));
     }
-    EpilogueArgs ep{P, ldp, source_features, target_features, D, ldd, lambda * lambda_scale, out_scale, U, V, out,
-                    ldo};
+    EpilogueArgs ep{P,   ldp, source_features, target_features, D, ldd, lambda * lambda_scale, out_scale, U, V, out,
+                    ldo, reinterpret_cast<float2*>(column_partials), ldc};
     {
         LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
-        gradient_kernel<<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt, ldt,
-                                                            static_cast<int>(n), ep);
+        if (column_partials != nullptr)
+            gradient_kernel<true><<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt, ldt,
+                                                                      static_cast<int>(n), ep);
+        else
+            gradient_kernel<false><<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt, ldt,
+                                                                       static_cast<int>(n), ep);
         FUGAL_TRY(launch_check("fugal_fw_gradient: (A P) B + epilogue"));
     }
     return FUGAL_OK;
+}
+
+}  // namespace
+
+extern "C" fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices,
+                                          const int32_t* b_row_pointers, const int32_t* b_col_indices,
+                                          const float* P, int64_t ldp, const float* source_features,
+                                          const float* target_features, const float* D, int64_t ldd,
+                                          double lambda, double lambda_scale, double out_scale, const double* U,
+                                          const double* V, float* out, int64_t ldo, void* workspace,
+                                          size_t workspace_bytes, fugal_stream_t stream) {
+    return fw_gradient(n, a_row_pointers, a_col_indices, b_row_pointers, b_col_indices, P, ldp, source_features,
+                       target_features, D, ldd, lambda, lambda_scale, out_scale, U, V, out, ldo, workspace,
+                       workspace_bytes, nullptr, 0, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" fugal_status fugal_gradient_column_chunks(int64_t n, int32_t* chunks) {
+    if (chunks == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_gradient_column_chunks: null output");
+    if (n <= 0 || n > (1ll << 30)) return fail(FUGAL_BAD_SHAPE, "fugal_gradient_column_chunks: bad n");
+    *chunks = static_cast<int32_t>((n + kTileCols - 1) / kTileCols);
+    return FUGAL_OK;
+}
+
+extern "C" fugal_status fugal_fw_gradient_column_stats(
+    int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices, const int32_t* b_row_pointers,
+    const int32_t* b_col_indices, const float* P, int64_t ldp, const float* source_features,
+    const float* target_features, const float* D, int64_t ldd, double lambda, double lambda_scale, double out_scale,
+    const double* U, const double* V, float* out, int64_t ldo, void* workspace, size_t workspace_bytes,
+    float* column_partials, int64_t ldc, fugal_stream_t stream) {
+    if (column_partials == nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_fw_gradient_column_stats: null column partials");
+    return fw_gradient(n, a_row_pointers, a_col_indices, b_row_pointers, b_col_indices, P, ldp, source_features,
+                       target_features, D, ldd, lambda, lambda_scale, out_scale, U, V, out, ldo, workspace,
+                       workspace_bytes, column_partials, ldc, reinterpret_cast<cudaStream_t>(stream));
 }

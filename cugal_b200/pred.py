@@ -17,6 +17,7 @@ CUDA devices are supported; a CPU config raises.
 
 from __future__ import annotations
 
+import ctypes
 import time
 from dataclasses import dataclass, field
 
@@ -90,6 +91,12 @@ class FrankWolfeEngine:
             self.solver = StandardSolver(n, self.config, dev)
         else:
             self.solver = SinkhornSolver(n, self.config, dev)
+            # column statistics of the cost, written by the gradient for the solve's
+            # first column update: (chunks, ld) (max, sum) pairs
+            chunks = ctypes.c_int32()
+            N.call("fugal_gradient_column_chunks", n, ctypes.byref(chunks))
+            self.colpart = torch.empty((chunks.value, 2 * self.ld), dtype=torch.float32, device=dev)
+            self.colpart_valid = False
         self.records = torch.empty((max(1, self.max_solves), N.RECORD_BYTES), dtype=torch.uint8, device=dev)
         self.solves = 0
         self.updates = 0
@@ -121,14 +128,22 @@ class FrankWolfeEngine:
             C = self.gradient(lam, out_scale=1.0, out=self.cost32, absorbed=False)
             exp_scale(C, -1.0 / reg, self.K_buf)
             return C
+        to_cost = out is None
         out = self.cost32 if out is None else out
         scale = (-1.0 / reg) if out_scale is None else out_scale
-        N.call("fugal_fw_gradient", self.n, self.A.row_pointers.data_ptr(), self.A.col_indices.data_ptr(),
-               self.B.row_pointers.data_ptr(), self.B.col_indices.data_ptr(), self.P_buf.data_ptr(), self.ld,
-               N.ptr(self.fs), N.ptr(self.ft), N.ptr(self.D), self.n if self.D is not None else 0,
-               float(lam), self.lambda_scale, scale, N.ptr(self.U) if absorbed else None,
-               N.ptr(self.V) if absorbed else None, out.data_ptr(), N.matrix_ld(out, "out"),
-               self.grad_ws.data_ptr(), self.grad_ws.numel(), N.stream_handle(self.device))
+        args = (self.n, self.A.row_pointers.data_ptr(), self.A.col_indices.data_ptr(),
+                self.B.row_pointers.data_ptr(), self.B.col_indices.data_ptr(), self.P_buf.data_ptr(), self.ld,
+                N.ptr(self.fs), N.ptr(self.ft), N.ptr(self.D), self.n if self.D is not None else 0,
+                float(lam), self.lambda_scale, scale, N.ptr(self.U) if absorbed else None,
+                N.ptr(self.V) if absorbed else None, out.data_ptr(), N.matrix_ld(out, "out"),
+                self.grad_ws.data_ptr(), self.grad_ws.numel())
+        if to_cost and not self.standard:
+            # the solve input: also hand the solve its first column update
+            N.call("fugal_fw_gradient_column_stats", *args, self.colpart.data_ptr(), self.ld,
+                   N.stream_handle(self.device))
+            self.colpart_valid = True
+        else:
+            N.call("fugal_fw_gradient", *args, N.stream_handle(self.device))
         return out
 
     def solve(self) -> int:
@@ -138,7 +153,9 @@ class FrankWolfeEngine:
         if self.standard:
             self.solver.solve(self.K_buf, self.u, self.v, self.records[k].data_ptr())
         else:
-            self.solver.solve(self.cost32, self.u, self.v, self.records[k].data_ptr())
+            self.solver.solve(self.cost32, self.u, self.v, self.records[k].data_ptr(),
+                              self.colpart if self.colpart_valid else None)
+            self.colpart_valid = False
         self.solves += 1
         return k
 

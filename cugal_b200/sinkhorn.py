@@ -47,7 +47,8 @@ class SinkhornSolver:
         if self.stream_dtype != N.FUGAL_F32:
             self.cost16 = torch.zeros((n, self.ld16), dtype=config.stream_dtype, device=self.device)
 
-    def params(self, cost32: torch.Tensor, u_out: torch.Tensor, v_out: torch.Tensor, record_ptr: int | None):
+    def params(self, cost32: torch.Tensor, u_out: torch.Tensor, v_out: torch.Tensor, record_ptr: int | None,
+               column_partials: torch.Tensor | None = None):
         c = self.config
         p = N.SolveParams()
         p.n = self.n
@@ -66,13 +67,21 @@ class SinkhornSolver:
         p.u_out = u_out.data_ptr()
         p.v_out = v_out.data_ptr()
         p.record = record_ptr
+        if column_partials is not None:
+            # (chunks, 2 ld) float32 = chunks x ld (max, sum) pairs
+            p.column_partials = column_partials.data_ptr()
+            p.column_partial_chunks = column_partials.shape[0]
+            p.column_partial_ld = column_partials.shape[1] // 2
         return p
 
-    def solve(self, cost32: torch.Tensor, u_out: torch.Tensor, v_out: torch.Tensor, record_ptr: int | None = None):
+    def solve(self, cost32: torch.Tensor, u_out: torch.Tensor, v_out: torch.Tensor, record_ptr: int | None = None,
+              column_partials: torch.Tensor | None = None):
         """One solve on the absorbed cost ``cost32`` (n x ld FP32): writes the dual
-        increments u_out, v_out (FP32) and, if given, a device solve record."""
+        increments u_out, v_out (FP32) and, if given, a device solve record.
+        ``column_partials``: the column statistics ``fugal_fw_gradient_column_stats``
+        wrote with this cost (skips the solve's own pass over it)."""
         N.require_cuda(cost32, "cost32", torch.float32)
-        p = self.params(cost32, u_out, v_out, record_ptr)
+        p = self.params(cost32, u_out, v_out, record_ptr, column_partials)
         N.call("fugal_sinkhorn_solve", ctypes.byref(p), self.workspace.data_ptr(), self.workspace.numel(),
                N.stream_handle(self.device))
 

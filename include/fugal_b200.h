@@ -248,6 +248,23 @@ fugal_status fugal_fw_gradient(int64_t n, const int32_t* a_row_pointers, const i
                                double out_scale, const double* U, const double* V, float* out, int64_t ldo,
                                void* workspace, size_t workspace_bytes, fugal_stream_t stream);
 
+/* fugal_fw_gradient that also hands the Sinkhorn solve its first column update
+ * (cugal/sinkhorn.py:105, v = -logsumexp over rows of K + u, u = 0 in the
+ * absorbed frame), so the solve does not read the cost for it: for every panel
+ * c of 128 output rows (c < chunks, fugal_gradient_column_chunks) and column j,
+ * column_partials[c * ldc + j] = (M, S) as two floats, M = max of out_ij log2 e
+ * over the panel's rows, S = sum of 2^(out_ij log2 e - M).  Pass the same
+ * buffer, chunks and ldc to fugal_sinkhorn_solve (column_partials fields). */
+fugal_status fugal_gradient_column_chunks(int64_t n, int32_t* chunks);
+fugal_status fugal_fw_gradient_column_stats(int64_t n, const int32_t* a_row_pointers,
+                                            const int32_t* a_col_indices, const int32_t* b_row_pointers,
+                                            const int32_t* b_col_indices, const float* P, int64_t ldp,
+                                            const float* source_features, const float* target_features,
+                                            const float* D, int64_t ldd, double lambda, double lambda_scale,
+                                            double out_scale, const double* U, const double* V, float* out,
+                                            int64_t ldo, void* workspace, size_t workspace_bytes,
+                                            float* column_partials, int64_t ldc, fugal_stream_t stream);
+
 /* No counterpart in the reference.  fugal_fw_gradient for callers that cannot
  * allocate device memory (a host whose device memory belongs to a pool allocator
  * every allocation must go through, or a binding that only passes input and
@@ -299,6 +316,12 @@ typedef struct {
     float* u_out;
     float* v_out;
     void* record; /* fugal_solve_record* in device memory, or NULL */
+    /* Optional (NULL: the solve reads cost32 for it): base-2 column (max, sum)
+     * partials of cost32 from fugal_fw_gradient_column_stats, chunks x ldc
+     * float pairs, merged into the first column update. */
+    const float* column_partials;
+    int32_t column_partial_chunks;
+    int64_t column_partial_ld;
 } fugal_solve_params;
 
 typedef struct {

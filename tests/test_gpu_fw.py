@@ -60,6 +60,59 @@ def test_gradient_matches_oracle(n, lam, lscale):
     np.testing.assert_allclose(L, expect, rtol=0, atol=2e-3 + 1e-6 * np.abs(expect).max())
 
 
+@pytest.mark.parametrize("n", [64, 1000, 3000])
+def test_gradient_column_stats(n):
+    """fugal_fw_gradient_column_stats writes the same cost as fugal_fw_gradient, and
+    its (max, sum) partials merge to the column log-sum-exp of that cost; a solve
+    fed the partials matches one that reads the cost for its first column update."""
+    import ctypes
+    from cugal_b200 import _native as N
+    from cugal_b200.adjacency import Adjacency
+    from cugal_b200.config import Config, SinkhornMethod
+    from cugal_b200.feature_extraction import Features
+    from cugal_b200.pred import FrankWolfeEngine
+    from cugal_b200.sinkhorn import read_record
+    g, h, _ = _pair(n, n + 1)
+    A, B = Adjacency.from_graph(g, "cuda"), Adjacency.from_graph(h, "cuda")
+    rng = np.random.default_rng(3)
+    feats = Features(torch.tensor(rng.random((n, 4)) * 5, dtype=torch.float32, device="cuda"),
+                     torch.tensor(rng.random((n, 4)) * 5, dtype=torch.float32, device="cuda"))
+    cfg = Config(device="cuda", dtype=torch.float32, sinkhorn_method=SinkhornMethod.LOG, use_sparse_adjacency=True,
+                 sinkhorn_regularization=0.05, sinkhorn_iterations=60, sinkhorn_threshold=1e-9, sinkhorn_eval_freq=10)
+    eng = FrankWolfeEngine(A, B, feats, cfg, max_solves=2)
+    eng.P_buf[:, :n] = torch.tensor(rng.random((n, n)) / n, dtype=torch.float32, device="cuda")
+    eng.U.copy_(torch.tensor(rng.standard_normal(n) * 30, device="cuda"))
+    eng.V.copy_(torch.tensor(rng.standard_normal(n) * 30, device="cuda"))
+    plain = eng.gradient(2, out=torch.zeros_like(eng.P_buf))  # fugal_fw_gradient
+    eng.gradient(2)                                            # the column-stats variant, into cost32
+    assert eng.colpart_valid
+    torch.cuda.synchronize()
+    assert torch.equal(plain[:, :n], eng.cost32[:, :n])
+    chunks = ctypes.c_int32()
+    N.call("fugal_gradient_column_chunks", n, ctypes.byref(chunks))
+    assert chunks.value == (n + 127) // 128 == eng.colpart.shape[0]
+    part = eng.colpart.view(chunks.value, eng.ld, 2)[:, :n].double().cpu().numpy()
+    M = part[..., 0].max(axis=0)
+    lse = (M + np.log2(np.sum(part[..., 1] * np.exp2(part[..., 0] - M), axis=0))) * np.log(2)
+    cost = eng.cost32[:, :n].double().cpu().numpy()
+    cm = cost.max(axis=0)
+    ref = cm + np.log(np.sum(np.exp(cost - cm), axis=0))
+    np.testing.assert_allclose(lse, ref, rtol=0, atol=2e-5 * max(1.0, np.abs(ref).max()))
+    # the solve with the partials against the solve that reads cost32 for them
+    outs = []
+    for use in (True, False):
+        du = torch.zeros(n, dtype=torch.float32, device="cuda")
+        dv = torch.zeros(n, dtype=torch.float32, device="cuda")
+        rec = torch.empty(N.RECORD_BYTES, dtype=torch.uint8, device="cuda")
+        eng.solver.solve(eng.cost32, du, dv, rec.data_ptr(), eng.colpart if use else None)
+        outs.append((du.cpu().numpy(), dv.cpu().numpy(), read_record(rec.cpu())))
+    (u1, v1, r1), (u2, v2, r2) = outs
+    assert r1.iteration_count == r2.iteration_count
+    shift = np.mean(u1 - u2)  # duals are defined up to u + c, v - c
+    np.testing.assert_allclose(u1 - shift, u2, rtol=0, atol=1e-5 + 4e-6 * np.abs(u2).max())
+    np.testing.assert_allclose(v1 + shift, v2, rtol=0, atol=1e-5 + 4e-6 * np.abs(v2).max())
+
+
 def _solve_gpu(C, u0, v0, reg, max_iter, thr, freq, mstart=None, stream_dtype=None, polish=1, warmup=10,
                every=50):
     from cugal_b200 import _native as N
