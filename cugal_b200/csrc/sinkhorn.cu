@@ -284,7 +284,8 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     const int t = st->it;
     const float omega = static_cast<float>(st->omega);
     const bool momentum = omega != 1.0f;
-    const bool exact_only = st->exact_next != 0 || momentum;  // uniform
+    // the absorb sweep always takes the exact path: it writes the copy centred on the row maximum
+    const bool exact_only = ABSORB || st->exact_next != 0 || momentum;  // uniform
     const uint32_t row_bytes = static_cast<uint32_t>(ncopy) * sizeof(T);
     const size_t stage_bytes = static_cast<size_t>(R) * p.slice_w * sizeof(T);
     const float* b_prev = p.b_buf + ((t - 1) & 1) * p.n_pad;
@@ -402,6 +403,9 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
 #pragma unroll
         for (int r = 0; r < R; ++r) a_old[r] = (r < rows) ? a_s[bt * R + r] : 0.f;
         bool fast_ok = false;
+        float off[R];  // ABSORB: row offset (nats) folded into the reduced-precision copy
+#pragma unroll
+        for (int r = 0; r < R; ++r) off[r] = 0.f;
         if (!exact_only) {
             // ---- fast path: exponents relative to the previous row normaliser -a_old:
             //      e = 2^(L log2e + b2 + a_old log2e)
@@ -501,13 +505,34 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                 alive = false;
                 break;
             }
-            if (!ABSORB) release(bt);
+            release(bt);  // the stage is not read again: x stays in registers
             float M2[R], sm[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 M2[r] = slot_max<THREADS, R>(xch, slot, C, r);
                 const float base = (M2[r] == -INFINITY) ? 0.f : M2[r];
                 const float2 nb = make_float2(-base, -base);
+                if (ABSORB && r < rows) {
+                    // cost16 = cost32 + b_j - max_j (cost32 + b_j): the row's largest entry is 0,
+                    // so the entries that carry its mass get the finest rounding; rounded once
+                    off[r] = base * kLn2;
+                    TOUT* dst = static_cast<TOUT*>(p.out16) + static_cast<size_t>(r0 + r) * p.ld16 + col0;
+#pragma unroll
+                    for (int g = 0; g < G; ++g) {
+                        const int c = (g * THREADS + tid) * V;
+                        if (c < ncopy) {
+                            TOUT o[V];
+#pragma unroll
+                            for (int q = 0; q < VP; ++q) {
+                                const float2 x = e[r][g * VP + q];
+                                o[2 * q] = from_float<TOUT>(c + 2 * q < nvalid ? (x.x - base) * kLn2 : -INFINITY);
+                                o[2 * q + 1] =
+                                    from_float<TOUT>(c + 2 * q + 1 < nvalid ? (x.y - base) * kLn2 : -INFINITY);
+                            }
+                            *reinterpret_cast<uint2*>(dst + c) = *reinterpret_cast<const uint2*>(o);
+                        }
+                    }
+                }
                 float2 ss = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
@@ -532,13 +557,17 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
             }
         }
         if (rank == 0 && tid < rows) {
-            float v = anew[0];
+            float v = anew[0], o = off[0];
 #pragma unroll
             for (int r = 1; r < R; ++r)
-                if (tid == r) v = anew[r];
+                if (tid == r) {
+                    v = anew[r];
+                    o = off[r];
+                }
             if (ABSORB) {
-                p.a_snap[r0 + tid] = v;
-                p.a[r0 + tid] = 0.f;
+                // frame of the copy: a = a_snap + a16 with a_snap = -(row offset)
+                p.a_snap[r0 + tid] = -o;
+                p.a[r0 + tid] = v + o;
             } else {
                 p.a[r0 + tid] = v;
             }
@@ -551,33 +580,6 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
 #pragma unroll
                 for (int h = 0; h < H; ++h) acc[h] = __ffma2_rn(e[r][h], w2, acc[h]);
             }
-        }
-        if (ABSORB) {
-            // cost16 = cost32 + b_j + a_i  (~ log P after this row update), rounded once
-#pragma unroll
-            for (int g = 0; g < G; ++g) {
-                const int c = (g * THREADS + tid) * V;
-                if (c < ncopy) {
-#pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        if (r < rows) {
-                            const uint4 raw =
-                                *reinterpret_cast<const uint4*>(stage + static_cast<size_t>(r) * p.slice_w + c);
-                            float vals[V];
-                            Vec<T>::unpack(raw, vals);
-                            TOUT o[V];
-#pragma unroll
-                            for (int q = 0; q < V; ++q)
-                                o[q] = from_float<TOUT>((c + q < nvalid) ? vals[q] + b_s[c + q] * kLn2 + anew[r]
-                                                                         : -INFINITY);
-                            TOUT* dst = static_cast<TOUT*>(p.out16) + static_cast<size_t>(r0 + r) * p.ld16 + col0 + c;
-                            *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(o);
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-            release(bt);
         }
     }
 
