@@ -371,6 +371,9 @@ def run_ours(args):
     # time of every launch of the family (the few that return at once included) over the sweeps that ran
     achieved = bytes_per * real / (ms / 1e3) / 1e9 if real else None
     traffic = traffic_per_launch(n, ld) if sdt is not None else None
+    # the row-owned kernel runs 512 threads per CTA without clusters; the cluster sweep at most 256
+    row_owned = sdt is not None and plan.get("threads") == 512 and plan.get("cluster") == 1
+    kernel_name = f"{'row_sweep_kernel' if row_owned else 'sweep_kernel'}<{args.stream_dtype}>"
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -406,7 +409,7 @@ def run_ours(args):
             "mean_sinkhorn_iterations": mean_sweeps, "sinkhorn_final_error": final_err,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "kernel": f"sweep_kernel<{args.stream_dtype}>", "launches": nl, "sweeps_run": real,
+                         "kernel": kernel_name, "launches": nl, "sweeps_run": real,
                          "avg_launch_ms": ms / real if real else None, "bytes_per_launch": bytes_per,
                          "peak_kind": peak_kind, "launch_shape": plan},
             "kernel_times_ms": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in fam.items()},
