@@ -1,10 +1,13 @@
 """Configuration of the FUGAL alignment (drop-in superset of cuGAL's ``Config``).
 
 Mirrors ``cugal/config.py:11-141`` of the reference: every field keeps its name,
-type and default, and ``to_dict``/``from_dict`` round-trip the same dictionary
-format, so result files written by either side load on the other.  Fields added
-here are appended after the reference's fields and default to behaviour that
-does not change the reference's algorithm.
+type and default, and ``to_dict``/``from_dict`` use the same dictionary format.
+``from_dict`` reads the reference's dictionaries (fields it does not know are
+dropped); the reference's ``from_dict`` accepts only its own fields, so result
+files store ``split_dict()``: the reference's fields, and the fields added here
+under a key of their own (``results.py``).  Fields added here are appended after
+the reference's fields and default to behaviour that does not change the
+reference's algorithm.
 """
 
 from __future__ import annotations
@@ -108,6 +111,12 @@ class Config:
         """Convert tensor to the configured dtype and device."""
         return input.to(dtype=self.dtype, device=self.device)
 
+    def split_dict(self) -> tuple[dict, dict]:
+        """(the reference's fields, the fields added here) of ``to_dict()``."""
+        d = self.to_dict()
+        ref = {k: d[k] for k in REFERENCE_FIELDS}
+        return ref, {k: v for k, v in d.items() if k not in ref}
+
     def to_dict(self) -> dict:
         config_dict = dataclasses.asdict(self)
         config_dict["dtype"] = _dtype_name(self.dtype)
@@ -126,3 +135,11 @@ class Config:
             config_dict["stream_dtype"] = getattr(torch, config_dict["stream_dtype"])
         known = {f.name for f in dataclasses.fields(cls)}
         return cls(**{k: v for k, v in config_dict.items() if k in known})
+
+
+# Field names of the reference's Config (cugal/config.py:55-120), in order.
+REFERENCE_FIELDS = ("safe_mode", "device", "dtype", "torch_sinkhorn", "sinkhorn_regularization", "sinkhorn_method",
+                    "sinkhorn_iterations", "dynamic_sinkhorn_regularization", "sinkhorn_scaling", "sinkhorn_threshold",
+                    "sinkhorn_eval_freq", "sinkhorn_momentum", "mu", "iter_count", "frank_wolfe_iter_count",
+                    "frank_wolfe_threshold", "use_sparse_adjacency", "sinkhorn_cache_size", "sinkhorn_momentum_start",
+                    "recompute_distance", "hungarian_method")

@@ -99,6 +99,18 @@ class Result:
         return cls(inter / nb if nb else 0.0, inter / na if na else 0.0, inter / den if den else 0.0,
                    alignment_accuracy(answer, mapping), profile)
 
+    def to_dict(self) -> dict:
+        """``benchmark/experiment.py:383-386``: the metrics plus ``profile.to_dict()``."""
+        return {"ics": self.ics, "ec": self.ec, "sss": self.sss, "accuracy": self.accuracy,
+                "profile": self.profile.to_dict()}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "Result":
+        from .profile import Profile
+        d = dict(d)
+        d["profile"] = Profile.from_dict(d["profile"])
+        return cls(**d)
+
     @staticmethod
     def average(results: list["Result"]) -> "Result":
         from .profile import Profile

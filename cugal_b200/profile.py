@@ -101,14 +101,19 @@ class Profile:
     def to_dict(self) -> dict:
         self.resolve()
         d = {f.name: getattr(self, f.name) for f in dataclasses.fields(self) if not f.name.startswith("_")}
-        d["sinkhorn_profiles"] = [dataclasses.asdict(p) for p in self.sinkhorn_profiles]
+        # the reference's SinkhornProfile fields only (its from_dict takes no others),
+        # so result files written here load there
+        d["sinkhorn_profiles"] = [{"errors": list(p.errors), "iteration_count": p.iteration_count, "time": p.time}
+                                  for p in self.sinkhorn_profiles]
         d["phase_times"] = {phase.value: t for phase, t in self.phase_times.items()}
         return d
 
     @classmethod
     def from_dict(cls, d: dict):
         d = dict(d)
-        d["sinkhorn_profiles"] = [SinkhornProfile(**p) for p in d["sinkhorn_profiles"]]
+        known = {f.name for f in dataclasses.fields(SinkhornProfile)}
+        d["sinkhorn_profiles"] = [SinkhornProfile(**{k: v for k, v in p.items() if k in known})
+                                  for p in d["sinkhorn_profiles"]]
         d["phase_times"] = {Phase[p]: t for p, t in d["phase_times"].items()}
         return cls(**d)
 
