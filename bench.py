@@ -346,6 +346,9 @@ def run_ours(args):
     import networkx as nx
     e2e_times = []
     h2d = 0
+    if args.e2e_steps:
+        # untimed warm-up call (first-use costs such as the pinned staging buffers of the P copy)
+        cugal(nx.Graph(src), nx.Graph(tgt), config, Profile())
     for _ in range(args.e2e_steps):
         s_copy, t_copy = nx.Graph(src), nx.Graph(tgt)
         h2d = (edge_array(s_copy).nbytes + edge_array(t_copy).nbytes)

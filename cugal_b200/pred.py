@@ -269,12 +269,61 @@ def hungarian(quasi_permutation: torch.Tensor, config: Config, profile: Profile)
     return cols
 
 
+_STAGE_BYTES = 256 << 20
+_COPY_THREADS = 8
+
+
+def matrix_to_host(M: torch.Tensor) -> np.ndarray:
+    """A new host numpy copy of the device matrix M (rows may be strided).
+
+    A plain ``M.cpu()`` copies into pageable memory at about 2 GB/s here (the
+    driver stages it and the fresh pages fault in one by one).  Instead, blocks of
+    rows go device -> pinned staging buffer (two 256 MB buffers from torch's
+    caching host allocator, so later calls reuse them) on a side stream, and
+    host threads move each block into the numpy array while the next block is
+    in flight."""
+    from concurrent.futures import ThreadPoolExecutor
+    n_rows, n_cols = M.shape
+    out = np.empty((n_rows, n_cols), dtype=np.float32)
+    if n_rows == 0 or n_cols == 0:
+        return out
+    rows = max(1, min(n_rows, _STAGE_BYTES // (n_cols * 4)))
+    stages = [torch.empty((rows, n_cols), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    copy_stream = torch.cuda.Stream(device=M.device)
+    copy_stream.wait_stream(torch.cuda.current_stream(M.device))
+    done = [torch.cuda.Event() for _ in range(2)]
+    pending = [None, None]
+
+    def host_copy(pool, k, r0, r1):
+        done[k].synchronize()
+        src = stages[k].numpy()
+        bounds = np.linspace(r0, r1, _COPY_THREADS + 1).astype(int)
+        parts = [pool.submit(np.copyto, out[a:b], src[a - r0:b - r0]) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
+        for f in parts:
+            f.result()
+
+    with ThreadPoolExecutor(max_workers=_COPY_THREADS + 1) as pool:
+        for blk, r0 in enumerate(range(0, n_rows, rows)):
+            k = blk & 1
+            r1 = min(n_rows, r0 + rows)
+            if pending[k] is not None:
+                pending[k].result()  # staging buffer k is free again
+            with torch.cuda.stream(copy_stream):
+                stages[k][:r1 - r0].copy_(M[r0:r1], non_blocking=True)
+                done[k].record(copy_stream)
+            pending[k] = pool.submit(host_copy, pool, k, r0, r1)
+        for f in pending:
+            if f is not None:
+                f.result()
+    return out
+
+
 def convert_to_permutation_matrix(quasi_permutation: torch.Tensor, config: Config,
                                   profile: Profile) -> tuple[np.ndarray, list[tuple[int, int]]]:
     """(P on the host, [(i, col[i])]) (``cugal/pred.py:181-193``)."""
     cols = hungarian(quasi_permutation, config, profile)
     mapping = [(i, int(c)) for i, c in enumerate(cols)]
-    return quasi_permutation.cpu().numpy(), mapping
+    return matrix_to_host(quasi_permutation), mapping
 
 
 def find_quasi_permutation_matrix(A: Adjacency, B: Adjacency, features: Features | torch.Tensor,
