@@ -309,7 +309,11 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
             }
         }
         // columns past n contribute 2^(-inf) = 0 without any masking in the hot loop
-        b_s[j] = j < nvalid ? b * kLog2e : -INFINITY;
+        // 16-bit rows (8 columns per 16-byte chunk): split layout, columns 8g..8g+3 at
+        // [4g, 4g+4) and 8g+4..8g+7 at [slice_w/2 + 4g, ...), so consecutive threads read
+        // consecutive 16 bytes (no bank conflicts); FP32 rows (4 per chunk) are already so
+        const int js = (V == 8) ? (((j & 7) < 4 ? 0 : p.slice_w / 2) + (j >> 3) * 4 + (j & 3)) : j;
+        b_s[js] = j < nvalid ? b * kLog2e : -INFINITY;
     }
     // Stage columns [ncopy, slice_w) are never written by the bulk copies: zero
     // them once so that they hold finite values (their b_s is -inf).
@@ -375,7 +379,8 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     auto load_b2 = [&](int c, float2* b2) {
 #pragma unroll
         for (int q = 0; q < VP; q += 2) {
-            const float4 b4 = *reinterpret_cast<const float4*>(b_s + c + 2 * q);
+            const float4 b4 = *reinterpret_cast<const float4*>(
+                V == 8 ? b_s + (q == 0 ? 0 : p.slice_w / 2) + (c >> 3) * 4 : b_s + c + 2 * q);
             b2[q] = make_float2(b4.x, b4.y);
             b2[q + 1] = make_float2(b4.z, b4.w);
         }
@@ -694,7 +699,9 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             if (blockIdx.x == 0) b_out[j] = bj;
             b = bj * kLog2e;
         }
-        b_s[j] = b;
+        // split layout: columns 8g..8g+3 at [4g, 4g+4), 8g+4..8g+7 at [COVER/2 + 4g, ...), so the
+        // 16-byte reads of consecutive threads (8 columns each) are consecutive: no bank conflicts
+        b_s[((j & 7) < 4 ? 0 : COVER / 2) + (j >> 3) * 4 + (j & 3)] = b;
     }
     // stage memory starts finite (columns past n_copy are never copied)
     for (size_t k = tid; k < static_cast<size_t>(p.stages) * SEG; k += kRowThreads)
@@ -750,9 +757,9 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             }
         }
     };
-    auto b2_at = [&](int c, float2* b2) {
-        const float4 lo = *reinterpret_cast<const float4*>(b_s + c);
-        const float4 hi = *reinterpret_cast<const float4*>(b_s + c + 4);
+    auto b2_at = [&](int c, float2* b2) {  // c: a multiple of 8
+        const float4 lo = *reinterpret_cast<const float4*>(b_s + (c >> 3) * 4);
+        const float4 hi = *reinterpret_cast<const float4*>(b_s + COVER / 2 + (c >> 3) * 4);
         b2[0] = make_float2(lo.x, lo.y);
         b2[1] = make_float2(lo.z, lo.w);
         b2[2] = make_float2(hi.x, hi.y);
