@@ -273,22 +273,6 @@ _STAGE_BYTES = 256 << 20
 _COPY_THREADS = 8
 
 
-def _host_matrix(n_rows: int, n_cols: int) -> np.ndarray:
-    """Uninitialised FP32 host matrix; a large one lives in an anonymous mapping
-    advised for transparent huge pages, so filling it takes about 1/512 of the
-    page faults of 4 KB pages (the array keeps the mapping alive)."""
-    import mmap
-    nbytes = n_rows * n_cols * 4
-    if nbytes >= (64 << 20) and hasattr(mmap, "MADV_HUGEPAGE"):
-        buf = mmap.mmap(-1, nbytes, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
-        try:
-            buf.madvise(mmap.MADV_HUGEPAGE)
-        except OSError:
-            pass
-        return np.frombuffer(buf, dtype=np.float32).reshape(n_rows, n_cols)
-    return np.empty((n_rows, n_cols), dtype=np.float32)
-
-
 def matrix_to_host(M: torch.Tensor) -> np.ndarray:
     """A new host numpy copy of the device matrix M (rows may be strided).
 
@@ -300,7 +284,7 @@ def matrix_to_host(M: torch.Tensor) -> np.ndarray:
     in flight."""
     from concurrent.futures import ThreadPoolExecutor
     n_rows, n_cols = M.shape
-    out = _host_matrix(n_rows, n_cols)
+    out = np.empty((n_rows, n_cols), dtype=np.float32)
     if n_rows == 0 or n_cols == 0:
         return out
     rows = max(1, min(n_rows, _STAGE_BYTES // (n_cols * 4)))
