@@ -17,7 +17,9 @@
 // error, takes the stop / momentum decision on the device and leaves
 // log(colsum) for the next sweep, which applies it to v when it loads it (so a
 // momentum change at an evaluation point affects v_{t+1} as in the reference).
-// Only the first column update of a solve is a separate max-stabilised pass.
+// Only the first column update of a solve is separate: a max-stabilised merge
+// of per-panel column (max, sum) partials, which the gradient writes with the
+// cost (column_partials) or a pass over the cost computes (column_pass_kernel).
 //
 // Two sweep kernels share this structure.
 //   sweep_kernel (FP32 sweeps, the absorb sweep, and 16-bit sweeps wider than
@@ -35,10 +37,11 @@
 // Precision: the cost arrives "absorbed" (cost32 = K + U_i + V_j with the
 // previous solves' duals U, V folded in), so its entries are ~log P and the
 // duals handled here are small increments.  With a BF16/FP16 stream the solve
-// reads cost32 for the first sweeps, then an "absorb" sweep writes the reduced-
-// precision copy cost16 = cost32 + a_i + b_j (~ log P after the row update,
-// rounded once), re-absorbed from cost32 every reabsorb_every sweeps, and ends
-// with FP32 polish sweeps on cost32.  LSE, duals and sums are FP32; the
+// reads cost32 for the first fp32_warmup_sweeps sweeps (default none), then an
+// "absorb" sweep writes the reduced-precision copy cost16 = cost32 + b_j - m_i,
+// m_i the row maximum of cost32 + b_j (rounded once; the row dual a_i + m_i
+// carries on in the copy's frame), re-absorbed from cost32 every reabsorb_every
+// sweeps, and ends with FP32 polish sweeps on cost32.  LSE, duals and sums are FP32; the
 // convergence reduction and the step decisions are FP64.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>

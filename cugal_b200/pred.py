@@ -5,10 +5,12 @@ return value ``(P as a host numpy array, [(i, column_i)])``.  The Frank-Wolfe
 loop (``pred.py:89-148``) runs as three kernel-library calls per step, all
 asynchronous on the current CUDA stream:
 
-  gradient  ``fugal_fw_gradient``    -2 A P B + D + lambda (1 - 2P), written as the
-                                      absorbed Sinkhorn input K + U_i + V_j
+  gradient  ``fugal_fw_gradient_column_stats``  -2 A P B + D + lambda (1 - 2P), written
+                                      as the absorbed Sinkhorn input K + U_i + V_j, and the
+                                      solve's first column update
   solve     ``fugal_sinkhorn_solve``  whole log-domain solve, decisions on device
   update    ``fugal_fw_update``       P += alpha (q - P), FP64 duality gap, duals folded
+            (``fugal_fw_direction`` + ``fugal_fw_line_search_update`` with line_search)
 
 The host only waits inside a solve (to stop enqueuing sweeps after
 convergence) and, when ``frank_wolfe_threshold`` is set, for the gap.  Only

@@ -1,7 +1,7 @@
 """Log-domain Sinkhorn (reference ``cugal/sinkhorn.py:51-156``).
 
 ``SinkhornSolver`` drives ``fugal_sinkhorn_solve`` for one problem size: it owns
-the solve workspace and runs a whole solve -- column pass, fused sweeps with
+the solve workspace and runs a whole solve -- first column update, fused sweeps with
 on-device convergence decisions, optional reduced-precision streaming and FP32
 polish -- as one call on the current stream.
 
