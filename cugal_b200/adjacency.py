@@ -10,6 +10,7 @@ of every edge of an undirected graph, and builds the CSR on the device with
 
 from __future__ import annotations
 
+import itertools
 from dataclasses import dataclass
 
 import numpy as np
@@ -22,7 +23,19 @@ def edge_array(graph) -> np.ndarray:
     """int32 (x, y) pairs of ``nx.edges(graph)``, plus reversed pairs if undirected
     (``cugal/adjacency.py:50-55``)."""
     m = graph.number_of_edges()
-    flat = np.fromiter((v for e in graph.edges() for v in e), dtype=np.int64, count=2 * m).reshape(-1, 2)
+    flat = None
+    if not graph.is_directed() and not graph.is_multigraph():
+        # each undirected edge once as (min, max), read straight off the adjacency dicts
+        # (about a third faster than graph.edges(); the pairs are the same up to order and
+        # orientation, and the CSR build sorts and adds both directions anyway)
+        try:
+            flat = np.fromiter(itertools.chain.from_iterable(
+                (u, v) for u, nbrs in graph.adjacency() for v in nbrs if u <= v), dtype=np.int64, count=2 * m)
+        except TypeError:  # labels that do not compare: the generic path reports them
+            flat = None
+    if flat is None:
+        flat = np.fromiter((v for e in graph.edges() for v in e), dtype=np.int64, count=2 * m)
+    flat = flat.reshape(-1, 2)
     if not graph.is_directed():
         flat = np.concatenate([flat, flat[:, ::-1]], axis=0)
     if flat.size and (flat.min() < 0 or flat.max() >= graph.number_of_nodes()):

@@ -69,3 +69,18 @@ def test_device_overlap_large_graph_matches_oracle():
     Ad = nx.to_numpy_array(g, nodelist=range(n))
     Bd = nx.to_numpy_array(h, nodelist=range(n))
     assert got == O.alignment_overlap(Ad, Bd, answer, truth)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_edge_array_matches_edge_list(seed):
+    """The adjacency-walk edge extraction gives the same directed pairs as
+    graph.edges() plus reversals, self-loops included (CPU)."""
+    from cugal_b200.adjacency import edge_array
+    g = nx.gnm_random_graph(300, 1200, seed=seed)
+    g.add_edges_from([(5, 5), (17, 17)])
+    got = edge_array(g)
+    flat = np.array([e for e in g.edges()], dtype=np.int64)
+    want = np.concatenate([flat, flat[:, ::-1]])
+    assert got.dtype == np.int32 and got.shape == want.shape
+    key = lambda a: np.lexsort((a[:, 1], a[:, 0]))
+    np.testing.assert_array_equal(got[key(got)], want[key(want)].astype(np.int32))
