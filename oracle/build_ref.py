@@ -6,9 +6,10 @@ TEST INFRASTRUCTURE ONLY.  Builds cuGAL's pybind11 module ``cuda_kernels``
 (``-O3 --use_fast_math``, ``cuda_kernels/setup.py:19``) for sm_100, using
 torch's extension loader with an explicit source list and an out-of-tree build
 directory.  Nothing is written under the reference tree; the output
-``oracle/_ref/cuda_kernels*.so`` is git-ignored and travels to the GPU box with
-the rest of the tree, where ``oracle/ref_gpu.py`` loads it to time and
-cross-check the reference's FP32 GPU path.
+``oracle/_ref/cuda_kernels*.so`` is git-ignored (a build product, copied with
+the working tree to the machine that runs the GPU tests), where
+``oracle/ref_gpu.py`` loads it to time and cross-check the reference's FP32 GPU
+path.
 
     python oracle/build_ref.py [--reference /root/reference]
 """

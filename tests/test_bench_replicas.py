@@ -1,6 +1,6 @@
 """bench.py's multi-rank logic on CPU with world size 2 (gloo): the max-over-ranks
 timing and barrier that the replica bench uses, and the reference arm launched
-the way the driver launches it (torchrun), where rank 0 alone prints."""
+the way a multi-GPU run launches it (torchrun), where rank 0 alone prints."""
 
 import json
 import os
