@@ -290,7 +290,10 @@ def matrix_to_host(M: torch.Tensor) -> np.ndarray:
     if n_rows == 0 or n_cols == 0:
         return out
     rows = max(1, min(n_rows, _STAGE_BYTES // (n_cols * 4)))
-    stages = [torch.empty((rows, n_cols), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    try:
+        stages = [torch.empty((rows, n_cols), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    except RuntimeError:  # no page-locked memory to be had: the plain (slower) copy
+        return M.cpu().numpy()
     copy_stream = torch.cuda.Stream(device=M.device)
     copy_stream.wait_stream(torch.cuda.current_stream(M.device))
     done = [torch.cuda.Event() for _ in range(2)]
