@@ -78,7 +78,7 @@ def dist_env():
 def dist_init(world: int, backend: str):
     if world > 1 and not torch.distributed.is_initialized():
         import datetime
-        torch.distributed.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        torch.distributed.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=180))
 
 
 def barrier(world: int):
