@@ -55,6 +55,8 @@ def parse_args(argv=None):
     ap.add_argument("--n", type=int, default=None, help="override the workload size")
     ap.add_argument("--stream-dtype", choices=["bf16", "fp16", "fp32"], default="bf16")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--fp32-steps", type=int, default=2,
+                    help="timed alignments of the FP32-stream comparison arm (0: none)")
     ap.add_argument("--iter-count", type=int, default=None, help="override the lambda steps (smoke runs)")
     ap.add_argument("--sinkhorn-iterations", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
@@ -167,6 +169,18 @@ def cpu_sweep_seconds(n: int, budget_s: float) -> tuple[float, int, str]:
     return per_iter, threads, sample
 
 
+def iteration_basis(workload: str, n: int, solves: int) -> tuple[float, str]:
+    """Mean Sinkhorn iterations per solve for the CPU extrapolations: the FP64
+    restatement's own counts on this workload (the reference's CPU FP64 path with
+    its marginal check made non-mutating runs the same iterations), else the
+    sinkhorn_iterations cap."""
+    counts = fp64_sweep_counts(workload, n)
+    if counts is not None and len(counts) == solves:
+        return float(np.mean(counts)), (f"the FP64 restatement's per-solve iteration counts on this workload "
+                                        f"(mean {np.mean(counts):.2f}, {SWEEPS_FP64.name})")
+    return 500.0, "500 iterations per solve (no FP64 count record for this workload)"
+
+
 def cpu_alignment_seconds(n: int, solves: int, sweeps_per_solve: float, budget_s: float):
     per_iter, threads, sample = cpu_sweep_seconds(n, budget_s)
     total = per_iter * sweeps_per_solve * solves
@@ -221,27 +235,74 @@ def executed_sweeps(iteration_counts, config) -> dict:
     return out
 
 
-def reference_gpu_sample(n: int, solves: int, sweeps: float, iters: int = 20):
-    """Seconds per alignment of the reference's FP32 GPU Sinkhorn (its own kernels,
-    oracle/_ref), extrapolated from `iters` timed iterations at size n, or None."""
+def reference_gpu_sample(src, tgt, sweeps_total: int, solves: int, fw_steps: int = 2, sweeps_timed: int = 40):
+    """Seconds per alignment of the reference's FP32 GPU path on its own kernels
+    (oracle/_ref), or None: ``fw_steps`` whole Frank-Wolfe steps of the
+    reference loop (cugal/pred.py:119-141: ``sparse_gradient`` with two
+    adjacency_matmul launches, add_distance and regularize; ``solve_log`` with
+    the non-mutating marginal check, its solve stopped after ``sweeps_timed``
+    iterations; ``update_quasi_permutation_log``) on the workload's own graphs
+    and features from the uniform P, timed part by part, then extrapolated to
+    ``solves`` gradient/update pairs and ``sweeps_total`` Sinkhorn iterations."""
     from oracle import ref_gpu
     if not ref_gpu.available():
         return None
-    g = torch.Generator(device="cuda").manual_seed(0)
-    C = torch.rand((n, n), generator=g, device="cuda") * 4
-    u = torch.zeros(n, device="cuda")
-    v = torch.zeros(n, device="cuda")
-    ref_gpu.solve_log(C, u, v, 1e-3, 3, 0.0, 10)  # warm-up (includes the transposed copy)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ref_gpu.solve_log(C, u, v, 1e-3, iters, 0.0, 10)
-    torch.cuda.synchronize()
-    per_iter = (time.perf_counter() - t0) / iters
-    del C
+    from cugal_b200.adjacency import Adjacency
+    from cugal_b200.config import Config
+    from cugal_b200.feature_extraction import Features
+    dev = "cuda"
+    A = Adjacency.from_graph(src, dev)
+    B = Adjacency.from_graph(tgt, dev)
+    feats = Features.create(A, B, Config(device=dev, dtype=torch.float32, mu=1.0))
+    fs, ft = feats.source.float().contiguous(), feats.target.float().contiguous()
+    n = src.number_of_nodes()
+    P = torch.full((n, n), 1.0 / n, device=dev)
+    u = torch.zeros(n, device=dev)
+    v = torch.zeros(n, device=dev)
+    t_grad, t_solve, t_upd, its = [], [], [], []
+    for it in range(1, fw_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        G = ref_gpu.sparse_gradient((A.col_indices, A.row_pointers), (B.col_indices, B.row_pointers), P, (fs, ft), 0)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        K, u, v, k, _ = ref_gpu.solve_log(G, u, v, 1e-3, sweeps_timed, 1e-4, 10)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        ref_gpu.update(P, K, u, v, 2.0 / (2.0 + it), 1e-3)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        t_grad.append(t1 - t0)
+        t_solve.append((t2 - t1) / k)
+        t_upd.append(t3 - t2)
+        its.append(k)
+        del G, K
+    del P
     torch.cuda.empty_cache()
-    return {"value": per_iter * sweeps * solves, "unit": UNIT, "per_iteration_ms": per_iter * 1e3,
-            "sample": f"{iters} iterations of the reference's solve_log GPU loop (cugal/sinkhorn.py:99-116) on its "
-                      f"own kernels at n={n}, extrapolated to {solves} solves x {sweeps:g} iterations"}
+    # the first step includes one-time costs (module load, first launches): use the last
+    g, sw, up = t_grad[-1], t_solve[-1], t_upd[-1]
+    value = solves * (g + up) + sweeps_total * sw
+    return {"value": value, "unit": UNIT, "gradient_ms": g * 1e3, "per_iteration_ms": sw * 1e3, "update_ms": up * 1e3,
+            "sample": f"{fw_steps} Frank-Wolfe steps of the reference's FP32 GPU loop on its own kernels "
+                      f"(gradient: 2 adjacency_matmul + add_distance + regularize; solve_log, non-mutating check, "
+                      f"{sweeps_timed} iterations timed per solve; update_quasi_permutation_log) at n={n} on this "
+                      f"workload; alignment = {solves} x (gradient + update) + {sweeps_total} iterations "
+                      f"(the FP32 stream's count in this run)"}
+
+
+SWEEPS_FP64 = ROOT / "tests" / "golden" / "er32768_fp64_sweeps.json"
+
+
+def fp64_sweep_counts(workload: str, n: int):
+    """Per-solve Sinkhorn iteration counts of the FP64 restatement of the
+    reference (non-mutating marginal check) over the workload's full schedule,
+    from the committed record, or None."""
+    if not SWEEPS_FP64.exists():
+        return None
+    d = json.loads(SWEEPS_FP64.read_text())
+    if d.get("workload") != workload or d.get("n") != n:
+        return None
+    return d["sinkhorn_iterations"]
 
 
 def run_reference(args):
@@ -253,24 +314,82 @@ def run_reference(args):
     n = args.n or w.n
     iters = args.iter_count or w.iter_count
     solves = iters * 10
-    # The reference's convergence check mutates K (cugal/sinkhorn.py:67-74) and never
-    # passes, so its solve runs to sinkhorn_iterations (500) every time.
-    sweeps = args.sinkhorn_iterations or 500
-    vals = []
+    sweeps, basis = iteration_basis(w.name, n, solves)
+    vals, per_iter = [], []
     for _ in range(args.warmup):
         cpu_sweep_seconds(n, min(2.0, args.cpu_seconds / 4))
     threads, sample = 0, ""
     for _ in range(args.steps):
         v, threads, sample = cpu_alignment_seconds(n, solves, sweeps, args.cpu_seconds / max(1, args.steps))
         vals.append(v)
+        per_iter.append(v / (solves * sweeps))
     value = statistics.median(vals)
+    sample += f"; iteration basis: {basis}"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": w.name, "n": n, "solves": solves, "sweeps_per_solve": sweeps},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            # the reference as it ships: its marginal check rescales K in place
+            # (cugal/sinkhorn.py:67-74), never passes, and every solve runs 500 iterations
+            "as_shipped_500_iterations": {"value": statistics.median(per_iter) * solves * 500, "unit": UNIT},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def timed_alignments(A, B, config, steps: int, warmup: int, world: int, dev):
+    """W untimed then K timed alignments on device-resident graphs (CUDA events
+    on the current stream, barrier + synchronize on both sides); returns the
+    seconds per alignment (max over ranks), the last columns, the profiles,
+    per-family kernel times and this library's launches in the timed region."""
+    from cugal_b200 import Profile
+    from cugal_b200 import _native as N
+    from cugal_b200.pred import align
+    for _ in range(warmup):
+        align(A, B, config, Profile())
+    torch.cuda.synchronize()
+    barrier(world)
+    N.timing_reset()
+    N.timing_enable(True)
+    launches0 = N.launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    profiles = []
+    cols = None
+    for _ in range(steps):
+        prof = Profile()
+        _, cols, _ = align(A, B, config, prof)
+        profiles.append(prof)
+    stop.record()
+    torch.cuda.synchronize()
+    launches = N.launch_count() - launches0
+    N.timing_enable(False)
+    elapsed = max_over_ranks(start.elapsed_time(stop) / 1000.0, world, dev)
+    fam = {name: N.timing_query(k) for k, name in enumerate(N.KERNEL_FAMILY_NAMES)}
+    for p in profiles:
+        p.resolve()
+    return elapsed / steps, cols, profiles, fam, launches
+
+
+def e2e_seconds(src, tgt, config, steps: int, world: int, dev):
+    """Seconds per alignment through the public cugal() call from host graphs
+    (edge-list copies in, P and the mapping out), after one untimed call."""
+    import networkx as nx
+    from cugal_b200 import Profile, cugal
+    from cugal_b200.adjacency import edge_array
+    cugal(nx.Graph(src), nx.Graph(tgt), config, Profile())
+    times, h2d, mapping = [], 0, None
+    for _ in range(steps):
+        s_copy, t_copy = nx.Graph(src), nx.Graph(tgt)
+        h2d = edge_array(s_copy).nbytes + edge_array(t_copy).nbytes
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        _, mapping = cugal(s_copy, t_copy, config, Profile())
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    return max_over_ranks(statistics.median(times), world, dev), h2d, mapping
 
 
 def run_ours(args):
@@ -279,16 +398,15 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    from cugal_b200 import Profile, cugal
     from cugal_b200 import _native as N
-    from cugal_b200.adjacency import Adjacency, edge_array
-    from cugal_b200.pred import align
+    from cugal_b200.adjacency import Adjacency
     from cugal_b200.sinkhorn import padded_ld
     from cugal_b200.synthetic import config_for, make_pair, node_accuracy
 
-    sdt = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": None}[args.stream_dtype]
+    dtypes = {"bf16": torch.bfloat16, "fp16": torch.float16, "fp32": None}
+    sdt = dtypes[args.stream_dtype]
     src, tgt, perm, w = make_pair(args.workload, n=args.n)
-    over = {"stream_dtype": sdt, "device": f"cuda:{local}"}
+    over = {"device": f"cuda:{local}"}
     if args.iter_count:
         over["iter_count"] = args.iter_count
     if args.sinkhorn_iterations:
@@ -299,68 +417,46 @@ def run_ours(args):
         over["reabsorb_every"] = args.reabsorb_every
     if args.line_search:
         over["line_search"] = True
-    config = config_for(w, **over)
+    config = config_for(w, stream_dtype=sdt, **over)
     n = src.number_of_nodes()
     A = Adjacency.from_graph(src, config.device)
     B = Adjacency.from_graph(tgt, config.device)
     torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        align(A, B, config, Profile())
-    torch.cuda.synchronize()
-    barrier(world)
-
     clocks = ClockSampler(local)
     clocks.start()
-    N.timing_reset()
-    N.timing_enable(True)
-    launches0 = N.launch_count()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    start.record()
-    profiles = []
-    for _ in range(args.steps):
-        prof = Profile()
-        P, cols, count = align(A, B, config, prof)
-        profiles.append(prof)
-    stop.record()
-    torch.cuda.synchronize()
-    launches = N.launch_count() - launches0
-    N.timing_enable(False)
+    value, cols, profiles, fam, launches = timed_alignments(A, B, config, args.steps, args.warmup, world, dev)
     clk = clocks.stop()
-    elapsed = start.elapsed_time(stop) / 1000.0
-    elapsed = max_over_ranks(elapsed, world, dev)
-    fam = {name: N.timing_query(k) for k, name in enumerate(N.KERNEL_FAMILY_NAMES)}
-    cols_np = cols.cpu().numpy() if isinstance(cols, torch.Tensor) else np.asarray(cols)
-    accuracy = float(np.mean(cols_np == perm))
-    for p in profiles:
-        p.resolve()
+    accuracy = float(np.mean(cols.cpu().numpy() == perm)) if isinstance(cols, torch.Tensor) else \
+        float(np.mean(np.asarray(cols) == perm))
     sk = [p.iteration_count for p in profiles[-1].sinkhorn_profiles]
     mean_sweeps = float(np.mean(sk)) if sk else 0.0
     fe = np.array([p.final_error for p in profiles[-1].sinkhorn_profiles], dtype=np.float64)
     final_err = {"median": float(np.median(fe)), "max": float(np.max(fe)),
                  "above_threshold": int(np.sum(fe >= config.sinkhorn_threshold)),
                  "threshold": config.sinkhorn_threshold, "solves": int(fe.size)} if fe.size else None
-
-    # end-to-end through cugal() from host graphs
-    import networkx as nx
-    e2e_times = []
-    h2d = 0
+    e2e, h2d, mapping = (None, 0, None)
     if args.e2e_steps:
-        # untimed warm-up call (first-use costs such as the pinned staging buffers of the P copy)
-        cugal(nx.Graph(src), nx.Graph(tgt), config, Profile())
-    for _ in range(args.e2e_steps):
-        s_copy, t_copy = nx.Graph(src), nx.Graph(tgt)
-        h2d = (edge_array(s_copy).nbytes + edge_array(t_copy).nbytes)
-        torch.cuda.synchronize()
-        barrier(world)
-        t0 = time.perf_counter()
-        Ph, mapping = cugal(s_copy, t_copy, config, Profile())
-        torch.cuda.synchronize()
-        e2e_times.append(time.perf_counter() - t0)
-    e2e = max_over_ranks(statistics.median(e2e_times), world, dev) if e2e_times else None
+        e2e, h2d, mapping = e2e_seconds(src, tgt, config, args.e2e_steps, world, dev)
     d2h = n * n * 4 + n * 8
-    e2e_acc = node_accuracy(mapping, perm) if e2e_times else None
+    e2e_acc = node_accuracy(mapping, perm) if mapping is not None else None
+
+    # the FP32-stream path on the same workload: the comparison the metric names
+    fp32_arm = None
+    if sdt is not None and args.fp32_steps > 0:
+        config32 = config_for(w, stream_dtype=None, **over)
+        v32, cols32, prof32, fam32, _ = timed_alignments(A, B, config32, args.fp32_steps, 1, world, dev)
+        e32, _, map32 = e2e_seconds(src, tgt, config32, 1, world, dev) if args.e2e_steps else (None, 0, None)
+        sk32 = [p.iteration_count for p in prof32[-1].sinkhorn_profiles]
+        fp32_arm = {"value": v32, "unit": UNIT, "steps": args.fp32_steps, "warmup": 1,
+                    "node_accuracy": float(np.mean(cols32.cpu().numpy() == perm)),
+                    "e2e": {"value": e32, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                    "e2e_node_accuracy": node_accuracy(map32, perm) if map32 is not None else None,
+                    "mean_sinkhorn_iterations": float(np.mean(sk32)) if sk32 else 0.0,
+                    "total_sinkhorn_iterations": int(np.sum(sk32)),
+                    "speedup_of_this_line": v32 / value,
+                    "e2e_speedup_of_this_line": (e32 / e2e) if (e32 and e2e) else None,
+                    "kernel_times_ms": {k: {"launches": c, "ms": round(t, 3)} for k, (c, t) in fam32.items()}}
 
     ld = padded_ld(n)
     plan = N.sinkhorn_plan(n, N.STREAM_DTYPES[sdt])
@@ -378,23 +474,22 @@ def run_ours(args):
     row_owned = sdt is not None and plan.get("threads") == 512 and plan.get("cluster") == 1
     kernel_name = f"{'row_sweep_kernel' if row_owned else 'sweep_kernel'}<{args.stream_dtype}>"
 
+    solves = config.iter_count * config.frank_wolfe_iter_count
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        solves = config.iter_count * config.frank_wolfe_iter_count
-        v, cores, sample = cpu_alignment_seconds(n, solves, mean_sweeps or config.sinkhorn_iterations,
-                                                 args.cpu_seconds)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        sweeps, basis = iteration_basis(w.name, n, solves)
+        v, cores, sample = cpu_alignment_seconds(n, solves, sweeps, args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample + f"; iteration basis: {basis}"}
 
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        total32 = fp32_arm["total_sinkhorn_iterations"] if fp32_arm else int(np.sum(sk))
         try:
-            ref_gpu = reference_gpu_sample(n, config.iter_count * config.frank_wolfe_iter_count,
-                                           mean_sweeps or config.sinkhorn_iterations)
+            ref_gpu = reference_gpu_sample(src, tgt, total32, solves)
         except Exception as exc:  # the reference build is optional
             ref_gpu = {"unavailable": str(exc)[:200]}
 
     if rank == 0:
-        value = elapsed / args.steps
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1000.0, "higher_is_better": False, "scaling": "weak",
@@ -402,8 +497,8 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": w.name, "n": n, "edges_source": src.number_of_edges(),
                        "edges_target": tgt.number_of_edges(), "stream_dtype": args.stream_dtype,
-                       "fw_steps": config.iter_count * config.frank_wolfe_iter_count,
-                       "sinkhorn_iterations": config.sinkhorn_iterations, "reg": config.sinkhorn_regularization,
+                       "fw_steps": solves, "sinkhorn_iterations": config.sinkhorn_iterations,
+                       "reg": config.sinkhorn_regularization,
                        "fp32_warmup_sweeps": config.fp32_warmup_sweeps, "reabsorb_every": config.reabsorb_every,
                        "polish_sweeps": config.polish_sweeps, "line_search": config.line_search,
                        "lap": config.hungarian_method.value, "parallelism": f"replicas{world}",
@@ -416,6 +511,7 @@ def run_ours(args):
                          "avg_launch_ms": ms / real if real else None, "bytes_per_launch": bytes_per,
                          "peak_kind": peak_kind, "launch_shape": plan},
             "kernel_times_ms": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in fam.items()},
+            "fp32_path": fp32_arm,
             "cpu_baseline": cpu,
             "reference_gpu_fp32": ref_gpu,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -70,6 +70,7 @@ SIGNATURES = {
     "fugal_update_quasi_permutation_log": (_INT, [_P, _I64, _P, _I64, _P, _P, _I64, _F, _F, _P, _P]),
     "fugal_greedy_lap_workspace_size": (_INT, [_I64, _INT, POINTER(c_size_t)]),
     "fugal_greedy_lap": (_INT, [_P, _I64, _I64, _INT, _P, _INT, _INT, _P, _P, _SZ, _P]),
+    "fugal_sampled_lap": (_INT, [_P, _I64, _I64, _P, _P, _INT, _P, _P]),
     "fugal_exact_lap_workspace_size": (_INT, [_I64, POINTER(c_size_t)]),
     "fugal_exact_lap": (_INT, [_P, _I64, _I64, _INT, _I64, _P, _P, _P, _P, _SZ, _P]),
     "fugal_count_le": (_INT, [_P, _I64, _I64, _F, _P, _P]),

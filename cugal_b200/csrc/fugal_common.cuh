@@ -172,13 +172,15 @@ FUGAL_DEVICE bool mbar_try_wait(uint64_t* bar, uint32_t parity, uint32_t hint_ns
     return ok != 0;
 }
 // Bounded wait: returns false (and records FUGAL_DEVICE_TIMEOUT) if the phase
-// does not complete within kWaitLimitNs.
-FUGAL_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, uint32_t hint_ns = kSuspendHintNs) {
+// does not complete within limit_ns (0: kWaitLimitNs).
+FUGAL_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, uint32_t hint_ns = kSuspendHintNs,
+                            uint64_t limit_ns = 0) {
     if (mbar_try_wait(bar, parity, hint_ns)) return true;
+    const uint64_t limit = limit_ns != 0 ? limit_ns : kWaitLimitNs;
     const uint64_t t0 = global_timer_ns();
     for (uint32_t i = 0; i < kMaxPolls; ++i) {
         if (mbar_try_wait(bar, parity, hint_ns)) return true;
-        if (global_timer_ns() - t0 > kWaitLimitNs) break;
+        if (global_timer_ns() - t0 > limit) break;
     }
     report_error(err, FUGAL_DEVICE_TIMEOUT);
     return false;

@@ -364,9 +364,139 @@ LapWs lap_layout(int64_t n, int K, char* base) {
     return w;
 }
 
+// ---------------------------------------------------------------------------
+// MORE_RAND (cugal/greedy_lap.py:34-48): rows in a caller-given random order;
+// row r is masked by the free columns (row *= taken), and its column is the
+// first index j whose running sum of the masked row reaches x = total * u_k
+// (u_k the k-th draw of Python's random.random(), so that
+// random.uniform(0, total) = total * u_k).  One CTA walks the rows: a pass over
+// the row forms 32-column chunk sums (FP64, each an inclusive warp scan), a
+// block scan over them finds the chunk where the running sum reaches x, and one
+// warp scans that chunk again with the same operations for the column.  The
+// free-column mask is a bit set in shared memory.
+constexpr int kSampleThreads = 1024;
+constexpr int kMaxSampleN = 1 << 19;
+
+__device__ __forceinline__ double warp_inclusive_scan(double v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kSampleThreads) sampled_walk_kernel(float* P, long long ldp, int n,
+                                                                      const long long* order, const double* uniforms,
+                                                                      int mutate, long long* cols) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nch = (n + 31) / 32;
+    double* csum = reinterpret_cast<double*>(smem);        // [nch] chunk sums of the masked row
+    unsigned* taken = reinterpret_cast<unsigned*>(csum + nch);  // [nch] bit (j % 32) of word j / 32
+    __shared__ double wscan[32];
+    __shared__ double s_before, s_total;
+    __shared__ int s_chunk;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int c = tid; c < nch; c += kSampleThreads) taken[c] = 0u;
+    const int per = (nch + kSampleThreads - 1) / kSampleThreads;
+    const int c0 = min(nch, tid * per), c1 = min(nch, c0 + per);
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const long long r = order[k];
+        float* row = P + static_cast<size_t>(r) * ldp;
+        // chunk sums of row * free (the masked entries written back when mutating)
+        for (int c = warp; c < nch; c += kSampleThreads / 32) {
+            const int j = c * 32 + lane;
+            float v = 0.f;
+            if (j < n) {
+                v = row[j];
+                if ((taken[c] >> lane) & 1u) {
+                    v = v * 0.f;
+                    if (mutate) row[j] = v;
+                }
+            }
+            const double incl = warp_inclusive_scan(static_cast<double>(v));
+            if (lane == 31) csum[c] = incl;
+        }
+        __syncthreads();
+        // block exclusive scan of the per-thread chunk ranges
+        double ts = 0.0;
+        for (int c = c0; c < c1; ++c) ts += csum[c];
+        const double incl = warp_inclusive_scan(ts);
+        if (lane == 31) wscan[warp] = incl;
+        if (tid == 0) s_chunk = INT_MAX;
+        __syncthreads();
+        if (warp == 0) {
+            const double wv = wscan[lane];
+            const double wi = warp_inclusive_scan(wv);
+            wscan[lane] = wi - wv;
+        }
+        __syncthreads();
+        const double before = wscan[warp] + (incl - ts);
+        // the total is the running sum as the last thread forms it, so some chunk reaches x
+        double cum = before;
+        for (int c = c0; c < c1; ++c) cum += csum[c];
+        if (tid == kSampleThreads - 1) s_total = cum;
+        __syncthreads();
+        const double x = s_total * uniforms[k];
+        cum = before;
+        int found = INT_MAX;
+        for (int c = c0; c < c1; ++c) {
+            const double nxt = cum + csum[c];
+            if (x <= nxt) {
+                found = c;
+                break;
+            }
+            cum = nxt;
+        }
+        if (found != INT_MAX) atomicMin(&s_chunk, found);
+        __syncthreads();
+        if (found != INT_MAX && found == s_chunk) s_before = cum;
+        __syncthreads();
+        if (warp == 0) {
+            const int c = s_chunk == INT_MAX ? nch - 1 : s_chunk;
+            const int j = c * 32 + lane;
+            float v = 0.f;
+            if (j < n) {
+                v = row[j];
+                if ((taken[c] >> lane) & 1u) v = v * 0.f;
+            }
+            const double run = s_before + warp_inclusive_scan(static_cast<double>(v));
+            const unsigned hit = __ballot_sync(0xffffffffu, j < n && x <= run);
+            const int m = hit ? c * 32 + __ffs(hit) - 1 : min(n - 1, c * 32 + 31);
+            if (lane == 0) {
+                taken[m / 32] |= 1u << (m % 32);
+                cols[r] = m;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace fugal
 
 using namespace fugal;
+
+extern "C" fugal_status fugal_sampled_lap(float* P, int64_t ldp, int64_t n, const int64_t* order,
+                                          const double* uniforms, int mutate, int64_t* columns_out,
+                                          fugal_stream_t stream_) {
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    if (P == nullptr || order == nullptr || uniforms == nullptr || columns_out == nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "fugal_sampled_lap: null argument");
+    if (n <= 0 || n > kMaxSampleN) return fail(FUGAL_BAD_SHAPE, "fugal_sampled_lap: n must be in [1, %d]", kMaxSampleN);
+    if (ldp < n) return fail(FUGAL_BAD_SHAPE, "fugal_sampled_lap: ldp < n");
+    const size_t nch = static_cast<size_t>((n + 31) / 32);
+    const size_t smem = nch * (sizeof(double) + sizeof(unsigned));
+    FUGAL_TRY(cuda_check(cudaFuncSetAttribute(sampled_walk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(smem)),
+                         "fugal_sampled_lap: shared memory"));
+    LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
+    sampled_walk_kernel<<<1, kSampleThreads, smem, stream>>>(P, ldp, static_cast<int>(n),
+                                                             reinterpret_cast<const long long*>(order), uniforms,
+                                                             mutate, reinterpret_cast<long long*>(columns_out));
+    return launch_check("fugal_sampled_lap");
+}
 
 extern "C" fugal_status fugal_greedy_lap_workspace_size(int64_t n, int candidates, size_t* bytes) {
     if (bytes == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_greedy_lap_workspace_size: null output");

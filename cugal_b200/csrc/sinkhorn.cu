@@ -112,6 +112,7 @@ __device__ void decide(SolveState* st, double err) {
         st->polish_count += 1;
     }
     if (!stop && t + 1 >= st->max_it) stop = true;
+    if (st->status != 0) stop = true;  // a bounded wait timed out: end the phase
     if (stop) {
         st->done = 1;
         st->final_it = t;
@@ -628,8 +629,11 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
 // exchange, and each thread keeps the running column sums of its EPT columns
 // in tensor memory (TMEM lane 32 (warp % 4) + lane, columns (warp / 4) EPT ..).
 // Rows stream through shared memory in segments of up to 16384 elements
-// (32 KB) with bulk copies; the column duals (b log2 e) of the whole row sit in
-// shared memory.  Same arithmetic as sweep_kernel: fast path against the
+// (32 KB) with bulk copies.  The column duals (b log2 e) of the thread's
+// columns sit in TMEM next to its column sums (BT = true, columns
+// (THREADS / 128) EPT + (warp / 4) EPT ..), so shared memory serves only the
+// streamed cost and more stages fit; or, BT = false, in shared memory for the
+// whole row.  Same arithmetic as sweep_kernel: fast path against the
 // absorbed frame (one barrier per row), exact max-stabilised path (two more
 // barriers) for exact sweeps and for rows whose sum leaves (1e-30, 1e30).
 // Waits are bounded; a timed-out wait is agreed at the next barrier
@@ -651,9 +655,24 @@ struct RowArgs {
     float* partials;     // [ctas][n_pad]
     long long n_pad;
     SolveState* st;
+    // Failure-detection test hooks (host environment, see make_row_args): the
+    // limit of every bounded wait (0: the 2 s default), and a local row of CTA 0
+    // whose first copy is armed for 16 bytes more than it delivers (-1: none),
+    // so that the waits on it time out.
+    unsigned long long wait_limit_ns;
+    int fault_row;
 };
 
-template <typename T, int EPT, int THREADS>
+// Sum of the 16 per-warp row partials, in a fixed pairwise order (every thread
+// computes the bit-identical value).
+__device__ __forceinline__ float sum16(const float* r) {
+    const float4 a = reinterpret_cast<const float4*>(r)[0], b = reinterpret_cast<const float4*>(r)[1];
+    const float4 c = reinterpret_cast<const float4*>(r)[2], d = reinterpret_cast<const float4*>(r)[3];
+    return (((a.x + a.y) + (a.z + a.w)) + ((b.x + b.y) + (b.z + b.w))) +
+           (((c.x + c.y) + (c.z + c.w)) + ((d.x + d.y) + (d.z + d.w)));
+}
+
+template <typename T, int EPT, int THREADS, bool BT>
 __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) {
     constexpr int kRowThreads = THREADS;
     constexpr int kRowWarps = THREADS / 32;
@@ -662,8 +681,10 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     constexpr int G = EPS / 8;                // 16-byte chunks per thread per segment
     constexpr int SEG = kRowThreads * EPS;    // elements per segment
     constexpr int H = EPT / 2;
-    constexpr uint32_t TCOLS = (THREADS / 128) * EPT;
+    constexpr uint32_t TCOLS = (BT ? 2 : 1) * (THREADS / 128) * EPT;
     static_assert(EPT % 16 == 0 && EPS % 8 == 0, "16-column TMEM chunks, 8-element loads");
+    static_assert(G % 2 == 0, "column duals load from TMEM 16 at a time");
+    static_assert(kRowWarps == 16, "sum16 reduces 16 warp partials");
     static_assert(SEG <= kRowSeg, "segment larger than a stage");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full[kMaxStages];
@@ -679,7 +700,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     const int n = p.n;
     constexpr int COVER = kRowThreads * EPT;  // columns the threads cover (>= n)
     float* b_s = reinterpret_cast<float*>(smem);
-    unsigned char* stage_base = smem + static_cast<size_t>(COVER) * 4;
+    unsigned char* stage_base = smem + (BT ? 0 : static_cast<size_t>(COVER) * 4);
     const size_t stage_bytes = static_cast<size_t>(SEG) * sizeof(T);
     const int row_begin = blockIdx.x * p.rows_per_cta;
     const int row_end = min(n, row_begin + p.rows_per_cta);
@@ -695,16 +716,18 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
 
     // column duals of this sweep, b = b_prev - w log(colsum_prev), kept as b log2 e;
     // -inf past n, so those columns contribute exactly 0
-    for (int j = tid; j < COVER; j += kRowThreads) {
-        float b = -INFINITY;
-        if (j < n) {
-            const float bj = b_prev[j] - omega * p.logcs[j];
-            if (blockIdx.x == 0) b_out[j] = bj;
-            b = bj * kLog2e;
+    if constexpr (!BT) {
+        for (int j = tid; j < COVER; j += kRowThreads) {
+            float b = -INFINITY;
+            if (j < n) {
+                const float bj = b_prev[j] - omega * p.logcs[j];
+                if (blockIdx.x == 0) b_out[j] = bj;
+                b = bj * kLog2e;
+            }
+            // split layout: columns 8g..8g+3 at [4g, 4g+4), 8g+4..8g+7 at [COVER/2 + 4g, ...), so the
+            // 16-byte reads of consecutive threads (8 columns each) are consecutive: no bank conflicts
+            b_s[((j & 7) < 4 ? 0 : COVER / 2) + (j >> 3) * 4 + (j & 3)] = b;
         }
-        // split layout: columns 8g..8g+3 at [4g, 4g+4), 8g+4..8g+7 at [COVER/2 + 4g, ...), so the
-        // 16-byte reads of consecutive threads (8 columns each) are consecutive: no bank conflicts
-        b_s[((j & 7) < 4 ? 0 : COVER / 2) + (j >> 3) * 4 + (j & 3)] = b;
     }
     // stage memory starts finite (columns past n_copy are never copied)
     for (size_t k = tid; k < static_cast<size_t>(p.stages) * SEG; k += kRowThreads)
@@ -722,6 +745,9 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     tmem_fence_after_sync();
     const uint32_t tcol = tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) +
                           static_cast<uint32_t>((warp >> 2) * EPT);
+    // this thread's column duals: element e (segment e / EPS, chunk (e % EPS) / 8) is column
+    // (e / EPS) SEG + (((e % EPS) / 8) THREADS + tid) 8 + e % 8
+    const uint32_t tb = tcol + static_cast<uint32_t>((THREADS / 128) * EPT);
     {
         float z[16];
 #pragma unroll
@@ -729,6 +755,29 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
 #pragma unroll
         for (int k = 0; k < EPT / 16; ++k) tmem_st16(tcol + 16 * k, z);
     }
+    if constexpr (BT) {
+#pragma unroll
+        for (int k = 0; k < EPT / 16; ++k) {
+            float bb[16];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int e = 16 * k + 8 * h;
+                const int c = (e / EPS) * SEG + (((e % EPS) / 8) * kRowThreads + tid) * 8;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    float b = -INFINITY;
+                    if (c + q < n) {
+                        const float bj = b_prev[c + q] - omega * p.logcs[c + q];
+                        if (blockIdx.x == 0) b_out[c + q] = bj;
+                        b = bj * kLog2e;
+                    }
+                    bb[8 * h + q] = b;
+                }
+            }
+            tmem_st16(tb + 16 * k, bb);
+        }
+    }
+    tmem_wait_st();
 
     auto issue = [&](int u) {
         const int s = u % p.stages;
@@ -736,7 +785,8 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         const int seg = u % NSEG;
         const int cols = min(SEG, p.n_copy - seg * SEG);
         const uint32_t bytes = cols > 0 ? static_cast<uint32_t>(cols) * sizeof(T) : 0u;
-        mbar_arrive_expect_tx(&full[s], bytes);
+        const uint32_t unmet = (blockIdx.x == 0 && u == p.fault_row * NSEG) ? 16u : 0u;
+        mbar_arrive_expect_tx(&full[s], bytes + unmet);
         if (bytes > 0)
             bulk_load(stage_base + s * stage_bytes,
                       static_cast<const T*>(p.L) + static_cast<size_t>(row) * p.ld + static_cast<size_t>(seg) * SEG,
@@ -768,6 +818,19 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         b2[2] = make_float2(hi.x, hi.y);
         b2[3] = make_float2(hi.z, hi.w);
     };
+    // Column duals of chunks g0 and g0 + 1 of segment sg (16 elements): from TMEM
+    // (BT), else from shared memory.  b2[8 * gg + q] holds columns 2q, 2q + 1 of chunk g0 + gg.
+    auto b_pair = [&](int sg, int g0, float2 (&b2)[8]) {
+        if constexpr (BT) {
+            float bb[16];
+            tmem_ld16(tb + sg * EPS + g0 * 8, bb);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) b2[q] = make_float2(bb[2 * q], bb[2 * q + 1]);
+        } else {
+            b2_at(sg * SEG + (g0 * kRowThreads + tid) * 8, b2);
+            b2_at(sg * SEG + ((g0 + 1) * kRowThreads + tid) * 8, b2 + 4);
+        }
+    };
 
     // Fast-path exponentials of local row rr (its stages waited for here):
     // yy = 2^(L log2e + b) against the absorbed frame, s2 / t2 partial row sums.
@@ -776,22 +839,27 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         for (int sg = 0; sg < NSEG; ++sg) {
             const int u = rr * NSEG + sg;
             okk = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
-                            p.suspend_ns) && okk;
+                            p.suspend_ns, p.wait_limit_ns) && okk;
             const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
 #pragma unroll
-            for (int g = 0; g < G; ++g) {
-                const int cl = (g * kRowThreads + tid) * 8;
-                float2 b2[4], v2[4];
-                b2_at(sg * SEG + cl, b2);
-                Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
+            for (int g0 = 0; g0 < G; g0 += 2) {
+                float2 b2[8];
+                b_pair(sg, g0, b2);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float2 e = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[q]));
-                    yy[(sg * EPS + g * 8) / 2 + q] = e;
-                    if (q & 1)
-                        t2 = __fadd2_rn(t2, e);
-                    else
-                        s2 = __fadd2_rn(s2, e);
+                for (int gg = 0; gg < 2; ++gg) {
+                    const int g = g0 + gg;
+                    const int cl = (g * kRowThreads + tid) * 8;
+                    float2 v2[4];
+                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 e = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[4 * gg + q]));
+                        yy[(sg * EPS + g * 8) / 2 + q] = e;
+                        if (q & 1)
+                            t2 = __fadd2_rn(t2, e);
+                        else
+                            s2 = __fadd2_rn(s2, e);
+                    }
                 }
             }
         }
@@ -842,9 +910,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                 bool in_range = true;
 #pragma unroll
                 for (int k = 0; k < RB; ++k) {
-                    S[k] = 0.f;
-#pragma unroll
-                    for (int w = 0; w < kRowWarps; ++w) S[k] += red_grp[par][k][w];
+                    S[k] = sum16(red_grp[par][k]);
                     if (k < nr && !(S[k] > 1e-30f && S[k] < 1e30f)) in_range = false;
                 }
                 if (!in_range) break;  // uniform
@@ -890,9 +956,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                 alive = false;
                 break;
             }
-            float S = 0.f;
-#pragma unroll
-            for (int w = 0; w < kRowWarps; ++w) S += red_s[par][w];
+            const float S = sum16(red_s[par]);
             fast_ok = S > 1e-30f && S < 1e30f;  // uniform
             if (fast_ok) {
                 release(r);
@@ -908,19 +972,24 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                 const int u = r * NSEG + sg;
                 if (exact_only)
                     ok = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
-                                   p.suspend_ns) && ok;
+                                   p.suspend_ns, p.wait_limit_ns) && ok;
                 const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
 #pragma unroll
-                for (int g = 0; g < G; ++g) {
-                    const int cl = (g * kRowThreads + tid) * 8;
-                    float2 b2[4], v2[4];
-                    b2_at(sg * SEG + cl, b2);
-                    Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
+                for (int g0 = 0; g0 < G; g0 += 2) {
+                    float2 b2[8];
+                    b_pair(sg, g0, b2);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float2 x = __ffma2_rn(v2[q], log2e2, b2[q]);
-                        y[(sg * EPS + g * 8) / 2 + q] = x;
-                        mx = fmaxf(mx, fmaxf(x.x, x.y));
+                    for (int gg = 0; gg < 2; ++gg) {
+                        const int g = g0 + gg;
+                        const int cl = (g * kRowThreads + tid) * 8;
+                        float2 v2[4];
+                        Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float2 x = __ffma2_rn(v2[q], log2e2, b2[4 * gg + q]);
+                            y[(sg * EPS + g * 8) / 2 + q] = x;
+                            mx = fmaxf(mx, fmaxf(x.x, x.y));
+                        }
                     }
                 }
             }
@@ -945,9 +1014,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             if (lane == 0) red_s[par][warp] = part;
             __syncthreads();
             release(r);
-            float S = 0.f;
-#pragma unroll
-            for (int w = 0; w < kRowWarps; ++w) S += red_s[par][w];
+            const float S = sum16(red_s[par]);
             const float lse = (M2 + log2f(S)) * kLn2;
             anew = momentum ? (1.f - omega) * p.a[row] - omega * lse : -lse;
             wr = (M2 == -INFINITY) ? 0.f : ex2(M2 + anew * kLog2e);
@@ -992,10 +1059,14 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             }
         }
     }
-    // a timed-out wait may leave copies in flight: wait for them (bounded)
+    // a timed-out wait may leave copies in flight: wait for each (bounded) before
+    // the shared memory they land in is released; the copies of different units
+    // complete on different stage barriers, so one that never completes does not
+    // hide the others
     if (!alive && tid == 0) {
         for (int u = r * NSEG; u < issued; ++u)
-            if (!mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status)) break;
+            mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status, kSuspendHintNs,
+                      p.wait_limit_ns);
     }
     tmem_fence_before_sync();
     __syncthreads();
@@ -1435,6 +1506,7 @@ fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_oc
 // kernel instead.
 struct RowPlan {
     bool use = false;
+    bool bt = true;
     int threads = 512;
     int ept = 0;
     int ctas = 0;
@@ -1446,15 +1518,36 @@ struct RowPlan {
 
 using RowKernelFn = void (*)(const RowArgs);
 
-template <typename T>
+template <typename T, bool BT>
 RowKernelFn row_kernel_typed(int ept) {
-    return ept == 16 ? row_sweep_kernel<T, 16, 512>
-                     : (ept == 32 ? row_sweep_kernel<T, 32, 512> : row_sweep_kernel<T, 64, 512>);
+    return ept == 16 ? row_sweep_kernel<T, 16, 512, BT>
+                     : (ept == 32 ? row_sweep_kernel<T, 32, 512, BT> : row_sweep_kernel<T, 64, 512, BT>);
 }
 
-RowKernelFn row_kernel_for(int dt, int ept, int threads) {
+RowKernelFn row_kernel_for(int dt, int ept, int threads, bool bt) {
     (void)threads;
-    return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16>(ept) : row_kernel_typed<__half>(ept);
+    if (bt) return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16, true>(ept) : row_kernel_typed<__half, true>(ept);
+    return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16, false>(ept) : row_kernel_typed<__half, false>(ept);
+}
+
+// Failure-detection test hooks of the row sweep, read from the environment at
+// each solve: FUGAL_TEST_WAIT_LIMIT_NS (limit of every bounded wait; unset: 2 s)
+// and FUGAL_TEST_FAULT_ROW (a local row of CTA 0 whose copy is armed for 16
+// bytes that never arrive, so the waits on it run out; unset: none).
+unsigned long long test_wait_limit_ns() {
+    const char* e = getenv("FUGAL_TEST_WAIT_LIMIT_NS");
+    return e != nullptr ? strtoull(e, nullptr, 10) : 0ull;
+}
+int test_fault_row() {
+    const char* e = getenv("FUGAL_TEST_FAULT_ROW");
+    return e != nullptr ? atoi(e) : -1;
+}
+
+// Column duals of the row sweep in TMEM (default) or shared memory
+// (FUGAL_ROW_DUALS_SMEM=1).
+bool row_duals_in_tmem() {
+    const char* e = getenv("FUGAL_ROW_DUALS_SMEM");
+    return !(e != nullptr && atoi(e) != 0);
 }
 
 // Threads per row-sweep CTA: 512.  (A 1024-thread CTA halves the columns per
@@ -1472,7 +1565,9 @@ fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool s
     rp.ept = static_cast<int>((n_pad + rp.threads * 16 - 1) / (rp.threads * 16)) * 16;  // 16, 32 or 64
     if (rp.ept == 48) rp.ept = 64;
     const size_t stage_bytes = static_cast<size_t>(rp.threads) * std::min(rp.ept, kRowSeg / rp.threads) * 2;
-    const size_t fixed = static_cast<size_t>(rp.threads) * rp.ept * 4;  // column duals of every covered column
+    rp.bt = row_duals_in_tmem();
+    // column duals of every covered column, unless they live in TMEM
+    const size_t fixed = rp.bt ? 0 : static_cast<size_t>(rp.threads) * rp.ept * 4;
     const int64_t room = static_cast<int64_t>(max_smem_optin()) - 1024 - static_cast<int64_t>(fixed);
     rp.stages = static_cast<int>(std::min<int64_t>(kMaxStages, room / static_cast<int64_t>(stage_bytes)));
     if (rp.stages < 2) return FUGAL_OK;
@@ -1481,7 +1576,7 @@ fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool s
     rp.rows_per_cta = static_cast<int>((n + ctas - 1) / ctas);
     rp.ctas = static_cast<int>((n + rp.rows_per_cta - 1) / rp.rows_per_cta);
     if (set_attributes) {
-        RowKernelFn fn = row_kernel_for(dt, rp.ept, rp.threads);
+        RowKernelFn fn = row_kernel_for(dt, rp.ept, rp.threads, rp.bt);
         FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp.smem),
                              "sinkhorn: row sweep shared memory"));
     }
@@ -1777,10 +1872,12 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
             ra.partials = w.partials;
             ra.n_pad = w.n_pad;
             ra.st = w.st;
+            ra.wait_limit_ns = test_wait_limit_ns();
+            ra.fault_row = test_fault_row();
             {
                 LaunchScope scope(FUGAL_KERNEL_SWEEP, stream);
-                row_kernel_for(p.stream_dtype, rowplan.ept, rowplan.threads)<<<rowplan.ctas, rowplan.threads, rowplan.smem,
-                                                                               stream>>>(ra);
+                row_kernel_for(p.stream_dtype, rowplan.ept, rowplan.threads, rowplan.bt)
+                    <<<rowplan.ctas, rowplan.threads, rowplan.smem, stream>>>(ra);
                 status = launch_check("sinkhorn: row sweep");
             }
             if (status == FUGAL_OK) status = finalize(rowplan.ctas);

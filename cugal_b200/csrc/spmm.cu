@@ -18,6 +18,10 @@
 // loads.  The grid walks output tiles panel-major (blockIdx.x = row tile,
 // blockIdx.y = 128-column panel), so the CTAs in flight share one panel of the
 // dense operand (n x 128 x 4 bytes, 16 MB at n = 32768) and the gathers hit L2.
+// The 32 x 128 output tile sits in shared memory as 16-byte chunks whose chunk
+// index is XOR-swizzled by (row mod 8): a warp stores a gathered row as one
+// 16-byte store per lane, and reads four columns of 32 rows (the transposed
+// orientation) as one 16-byte load per lane, both without bank conflicts.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,6 +35,14 @@ namespace fugal {
 constexpr int kTileRows = 32;     // gathered output rows per CTA
 constexpr int kTileCols = 128;    // columns per CTA (32 lanes x float4)
 constexpr int kSpmmThreads = 256; // 8 warps, 4 rows each
+constexpr int kChunks = kTileCols / 4;  // 16-byte chunks per tile row
+
+// The tile: kTileRows rows of kChunks float4 chunks; chunk q of row r is stored
+// at position q ^ (r & 7).
+struct Tile {
+    float4 c[kTileRows][kChunks];
+    __device__ __forceinline__ float4& at(int r, int q) { return c[r][q ^ (r & 7)]; }
+};
 
 // 4 consecutive floats of row k starting at column c: one 16-byte load when the
 // rows are 16-byte aligned (VEC), else scalar loads guarded by n.
@@ -88,11 +100,12 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
     return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
 
-// Fill tile[r][0..127] with the gathered rows r0 .. r0+31 of A X for columns c0 .. c0+127.
+// Fill the tile with the gathered rows r0 .. r0+31 of A X for columns c0 .. c0+127
+// (lane l: chunk l of each row).
 template <bool VEC>
 __device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const int* __restrict__ col,
                                             const float* __restrict__ X, long long ldx, int n, int r0, int c0,
-                                            float (*tile)[kTileCols + 1], float sign) {
+                                            Tile& tile, float sign) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c = c0 + lane * 4;
     const bool c_ok = c < n;
@@ -100,10 +113,7 @@ __device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const in
         const int row = r0 + rr;
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
         if (row < n) acc = gather_row<VEC>(rp, col, X, ldx, n, row, c, c_ok);
-        tile[rr][lane * 4 + 0] = sign * acc.x;
-        tile[rr][lane * 4 + 1] = sign * acc.y;
-        tile[rr][lane * 4 + 2] = sign * acc.z;
-        tile[rr][lane * 4 + 3] = sign * acc.w;
+        tile.at(rr, lane) = make_float4(sign * acc.x, sign * acc.y, sign * acc.z, sign * acc.w);
     }
 }
 
@@ -113,25 +123,40 @@ __global__ void __launch_bounds__(kSpmmThreads) spmm_kernel(const int* __restric
                                                             const float* __restrict__ X, long long ldx, int n,
                                                             float* __restrict__ out, long long ldo, int transpose,
                                                             float sign) {
-    __shared__ float tile[kTileRows][kTileCols + 1];
+    __shared__ Tile tile;
     const int r0 = blockIdx.x * kTileRows;
     const int c0 = blockIdx.y * kTileCols;
     gather_tile<VEC>(rp, col, X, ldx, n, r0, c0, tile, sign);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (transpose) {
-        // row c of out gets the 32 values tile[0..31][c - c0]
-        for (int cc = warp; cc < kTileCols; cc += kSpmmThreads / 32) {
-            const int cg = c0 + cc, rg = r0 + lane;
-            if (cg < n && rg < n) out[static_cast<size_t>(cg) * ldo + rg] = tile[lane][cc];
+        // rows c0+4q .. c0+4q+3 of out get the 32 values of columns 4q .. 4q+3 of the
+        // tile: lane l reads chunk q of tile row l
+        const int rg = r0 + lane;
+        for (int q = warp; q < kChunks; q += kSpmmThreads / 32) {
+            const float4 v = tile.at(lane, q);
+            const int cg = c0 + 4 * q;
+            if (rg < n) {
+                if (cg + 0 < n) out[static_cast<size_t>(cg + 0) * ldo + rg] = v.x;
+                if (cg + 1 < n) out[static_cast<size_t>(cg + 1) * ldo + rg] = v.y;
+                if (cg + 2 < n) out[static_cast<size_t>(cg + 2) * ldo + rg] = v.z;
+                if (cg + 3 < n) out[static_cast<size_t>(cg + 3) * ldo + rg] = v.w;
+            }
         }
     } else {
         for (int rr = warp; rr < kTileRows; rr += kSpmmThreads / 32) {
             const int rg = r0 + rr;
             if (rg >= n) continue;
-            for (int cc = lane; cc < kTileCols; cc += 32) {
-                const int cg = c0 + cc;
-                if (cg < n) out[static_cast<size_t>(rg) * ldo + cg] = tile[rr][cc];
+            const float4 v = tile.at(rr, lane);
+            const int cg = c0 + 4 * lane;
+            float* o = out + static_cast<size_t>(rg) * ldo + cg;
+            if (cg + 3 < n && (reinterpret_cast<uintptr_t>(o) & 15u) == 0) {
+                *reinterpret_cast<float4*>(o) = v;
+            } else {
+                if (cg + 0 < n) o[0] = v.x;
+                if (cg + 1 < n) o[1] = v.y;
+                if (cg + 2 < n) o[2] = v.z;
+                if (cg + 3 < n) o[3] = v.w;
             }
         }
     }
@@ -155,18 +180,21 @@ struct EpilogueArgs {
 };
 
 // Y = B Tt = (APB)^T over the tile (rows j0.., cols i0..), then the gradient
-// epilogue in (i, j) orientation.  COLSTATS: the CTA also reduces, for each of
-// its 32 output columns j, the 128 values it wrote over rows i0 .. i0+127 to a
-// base-2 (max, sum) pair, x = out log2 e: M = max x, S = sum 2^(x - M), stored
-// at colpart[blockIdx.y][j] (the first column update of the Sinkhorn solve
-// merges them instead of reading the cost again).
+// epilogue in (i, j) orientation: lane l takes j = j0 + l, and warp w the tile
+// columns i0 + 4q .. i0 + 4q + 3 for q = w, w + 8, w + 16, w + 24 (one 16-byte
+// tile read per q), so every global access is a 128-byte row segment.  The P
+// term is skipped when lambda is 0 (its factor).  COLSTATS: the CTA also
+// reduces, for each of its 32 output columns j, the 128 values it wrote over
+// rows i0 .. i0+127 to a base-2 (max, sum) pair, x = out log2 e: M = max x,
+// S = sum 2^(x - M), stored at colpart[blockIdx.y][j] (the first column update
+// of the Sinkhorn solve merges them instead of reading the cost again).
 template <bool COLSTATS>
-__global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __restrict__ rp,
+__global__ void __launch_bounds__(kSpmmThreads, 6) gradient_kernel(const int* __restrict__ rp,
                                                                 const int* __restrict__ col,
                                                                 const float* __restrict__ Tt, long long ldt, int n,
                                                                 const EpilogueArgs ep) {
     constexpr int kWarps = kSpmmThreads / 32;
-    __shared__ float tile[kTileRows][kTileCols + 1];
+    __shared__ Tile tile;
     __shared__ float4 fi[kTileCols];
     __shared__ float4 fj[kTileRows];
     __shared__ float2 cst[COLSTATS ? kWarps : 1][kTileRows];
@@ -187,40 +215,60 @@ __global__ void __launch_bounds__(kSpmmThreads) gradient_kernel(const int* __res
     const double vj = (ep.V && j < n) ? ep.V[j] : 0.0;
     const float4 f2 = has_f ? fj[lane] : make_float4(0, 0, 0, 0);
     const float lam = static_cast<float>(ep.lam);
+    const bool use_p = lam != 0.f;
     float xmax = -INFINITY;
-    for (int ii = warp; ii < kTileCols; ii += kWarps) {
-        const int i = i0 + ii;
-        if (i >= n || j >= n) break;
-        // The gradient itself in FP32, as the reference computes it (SpMM, distance,
-        // regularize: cugal/pred.py:54-74, distance.cu:11-53, regularize.cu:10-39) ...
-        const float apb = tile[lane][ii];
-        const float p = ep.P[static_cast<size_t>(i) * ep.ldp + j];
-        float g = __fadd_rn(__fmul_rn(-2.0f, apb), __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, p))));
-        if (has_f) {
-            const float4 f1 = fi[ii];
-            const float d0 = __fsub_rn(f1.x, f2.x), d1 = __fsub_rn(f1.y, f2.y);
-            const float d2 = __fsub_rn(f1.z, f2.z), d3 = __fsub_rn(f1.w, f2.w);
-            g = __fadd_rn(g, __fsqrt_rn(__fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))))));
-        } else if (ep.D != nullptr) {
-            g = __fadd_rn(g, ep.D[static_cast<size_t>(i) * ep.ldd + j]);
+    for (int q = warp; q < kChunks; q += kWarps) {
+        if (i0 + 4 * q >= n || j >= n) break;
+        const float4 apb4 = tile.at(lane, q);
+        const float apbs[4] = {apb4.x, apb4.y, apb4.z, apb4.w};
+        float xs[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int ii = 4 * q + t;
+            const int i = i0 + ii;
+            xs[t] = -INFINITY;
+            if (i >= n) continue;
+            // The gradient itself in FP32, as the reference computes it (SpMM, distance,
+            // regularize: cugal/pred.py:54-74, distance.cu:11-53, regularize.cu:10-39) ...
+            float reg = 0.f;
+            if (use_p) {
+                const float p = ep.P[static_cast<size_t>(i) * ep.ldp + j];
+                reg = __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, p)));
+            }
+            float g = __fadd_rn(__fmul_rn(-2.0f, apbs[t]), reg);
+            if (has_f) {
+                const float4 f1 = fi[ii];
+                const float d0 = __fsub_rn(f1.x, f2.x), d1 = __fsub_rn(f1.y, f2.y);
+                const float d2 = __fsub_rn(f1.z, f2.z), d3 = __fsub_rn(f1.w, f2.w);
+                g = __fadd_rn(g, __fsqrt_rn(__fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))))));
+            } else if (ep.D != nullptr) {
+                g = __fadd_rn(g, ep.D[static_cast<size_t>(i) * ep.ldd + j]);
+            }
+            // ... and its combination with the accumulated duals in FP64: the terms are
+            // O(1/reg) and cancel to O(1), which FP32 would not resolve.
+            const double ui = ep.U ? ep.U[i] : 0.0;
+            const float o = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + vj));
+            ep.out[static_cast<size_t>(i) * ep.ldo + j] = o;
+            xs[t] = o * kLog2e;
+            xmax = fmaxf(xmax, xs[t]);
         }
-        // ... and its combination with the accumulated duals in FP64: the terms are
-        // O(1/reg) and cancel to O(1), which FP32 would not resolve.
-        const double ui = ep.U ? ep.U[i] : 0.0;
-        const float o = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + vj));
-        ep.out[static_cast<size_t>(i) * ep.ldo + j] = o;
         if constexpr (COLSTATS) {
-            // the tile entry this thread just consumed keeps x = out log2 e for the sum below
-            const float x = o * kLog2e;
-            tile[lane][ii] = x;
-            xmax = fmaxf(xmax, x);
+            // the chunk this thread just consumed keeps x = out log2 e for the sum below
+            tile.at(lane, q) = make_float4(xs[0], xs[1], xs[2], xs[3]);
         }
     }
     if constexpr (COLSTATS) {
-        // second pass over the same tile entries (this thread's own, no barrier needed)
+        // second pass over the same tile chunks (this thread's own, no barrier needed);
+        // chunks past n hold -inf and add 0
         float sum = 0.f;
         if (xmax != -INFINITY) {
-            for (int ii = warp; ii < kTileCols && i0 + ii < n; ii += kWarps) sum += ex2(tile[lane][ii] - xmax);
+            for (int q = warp; q < kChunks && i0 + 4 * q < n; q += kWarps) {
+                const float4 x = tile.at(lane, q);
+                sum += ex2(x.x - xmax);
+                sum += ex2(x.y - xmax);
+                sum += ex2(x.z - xmax);
+                sum += ex2(x.w - xmax);
+            }
         }
         cst[warp][lane] = make_float2(xmax, sum);
         __syncthreads();

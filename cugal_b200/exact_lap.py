@@ -13,9 +13,11 @@ FUGAL_OK, FUGAL_ITER_LIMIT = 0, 4
 
 
 def default_max_steps(n: int) -> int:
-    """Cap on Dijkstra steps: 32 per row on average (a converged Frank-Wolfe P
-    needs about one per row)."""
-    return 32 * n + 1024
+    """Cap on Dijkstra steps: n per row, a bound no shortest-augmenting-path run
+    exceeds (each step of a row's search settles one more column), so reaching it
+    means a fault, not a hard instance.  A converged Frank-Wolfe P needs about one
+    step per row."""
+    return n * n + 1024
 
 
 def exact_assign(P: torch.Tensor, maximize: bool = True, max_steps: int | None = None):

@@ -24,7 +24,6 @@ import time
 from dataclasses import dataclass, field
 
 import numpy as np
-import scipy.optimize
 import scipy.sparse
 import scipy.sparse.csgraph
 import torch
@@ -33,7 +32,7 @@ from . import _native as N
 from .adjacency import Adjacency
 from .config import Config, HungarianMethod, SinkhornMethod
 from .feature_extraction import Features
-from .exact_lap import FUGAL_ITER_LIMIT, FUGAL_OK, exact_assign
+from .exact_lap import FUGAL_ITER_LIMIT, FUGAL_OK, default_max_steps, exact_assign
 from .greedy_lap import greedy_assign
 from .profile import Phase, Profile, SinkhornProfile, TimeStamp
 from .sinkhorn import SinkhornSolver, StandardSolver, exp_scale, padded_ld, read_record
@@ -230,7 +229,7 @@ def sparse_gradient(A: Adjacency, B: Adjacency, A_transpose, B_transpose, P: tor
 
 
 GREEDY_METHODS = (HungarianMethod.GREEDY, HungarianMethod.DOUBLE_GREEDY, HungarianMethod.PARALLEL_GREEDY,
-                  HungarianMethod.RAND)
+                  HungarianMethod.RAND, HungarianMethod.MORE_RAND)
 
 
 def round_on_device(P: torch.Tensor, config: Config, profile: Profile):
@@ -246,13 +245,15 @@ def round_on_device(P: torch.Tensor, config: Config, profile: Profile):
         cols, _, status = exact_assign(P, maximize=True)
         st = int(status.item())
         if st == FUGAL_ITER_LIMIT:
-            # the device search hit its step cap: scipy itself gives the same mapping
-            _, cols = scipy.optimize.linear_sum_assignment(P.cpu().numpy(), maximize=True)
-        elif st != FUGAL_OK:
+            raise N.NativeError(f"fugal_exact_lap: the search exceeded {default_max_steps(n)} Dijkstra steps, "
+                                "more than a shortest-augmenting-path run can take")
+        if st != FUGAL_OK:
             raise N.NativeError(f"fugal_exact_lap: device status {st}")
     elif method in GREEDY_METHODS:
         cols = greedy_assign(P, method, config.lap_candidates)
     elif method == HungarianMethod.SPARSE:
+        # the reference's own host algorithm (cugal/pred.py:170-177): scipy's sparse
+        # matching has tie rules of its own, which a device search would not share
         host = scipy.sparse.csr_matrix(P.cpu().numpy())
         _, cols = scipy.sparse.csgraph.min_weight_full_bipartite_matching(host, maximize=True)
     else:

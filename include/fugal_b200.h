@@ -146,6 +146,16 @@ fugal_status fugal_greedy_lap(float* P, int64_t ldp, int64_t n, int method, cons
                               int candidates, int mutate, int64_t* columns_out, void* workspace,
                               size_t workspace_bytes, fugal_stream_t stream);
 
+/* MORE_RAND rounding (cugal/greedy_lap.py:34-48, a Python loop of n launches with
+ * a host draw each): rows in the caller's order order[k]; row r is masked by the
+ * columns still free (row *= taken, written back when mutate != 0) and takes the
+ * first column j whose running sum of the masked row reaches total * uniforms[k]
+ * (uniforms[k]: the k-th random.random() draw, so total * uniforms[k] is the
+ * reference's random.uniform(0, cumsum[-1])).  Sums in FP64.  order: int64
+ * device array, uniforms: double device array, both of length n; n <= 2^19. */
+fugal_status fugal_sampled_lap(float* P, int64_t ldp, int64_t n, const int64_t* order, const double* uniforms,
+                               int mutate, int64_t* columns_out, fugal_stream_t stream);
+
 /* Exact assignment with the same mapping as scipy.optimize.linear_sum_assignment
  * (the reference's HungarianMethod.SCIPY rounding, cugal/pred.py:151-158): cost
  * c = -P (maximize != 0) or P, converted to double; Crouse's shortest augmenting

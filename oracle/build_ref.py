@@ -11,7 +11,7 @@ the working tree to the machine that runs the GPU tests), where
 ``oracle/ref_gpu.py`` loads it to time and cross-check the reference's FP32 GPU
 path.
 
-    python oracle/build_ref.py [--reference /root/reference]
+    python oracle/build_ref.py [--reference <cuGAL checkout>]
 """
 
 from __future__ import annotations
@@ -25,8 +25,13 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 
 
-def build(reference: str = "/root/reference", verbose: bool = False) -> Path | None:
-    src = Path(reference) / "cuda_kernels"
+def default_reference() -> str:
+    """``CUGAL_REFERENCE``, else a checkout named ``reference`` beside this repository."""
+    return os.environ.get("CUGAL_REFERENCE") or str(HERE.parent.parent / "reference")
+
+
+def build(reference: str | None = None, verbose: bool = False) -> Path | None:
+    src = Path(reference or default_reference()) / "cuda_kernels"
     if not src.exists():
         return None
     os.environ.setdefault("TORCH_CUDA_ARCH_LIST", "10.0")
@@ -43,7 +48,7 @@ def build(reference: str = "/root/reference", verbose: bool = False) -> Path | N
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("CUGAL_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=default_reference())
     ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args()
     out = build(a.reference, a.verbose)

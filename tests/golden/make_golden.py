@@ -1,7 +1,7 @@
 """Generate golden vectors by running the reference's own Python implementation.
 
-Run in a container that has the cuGAL reference checked out (default path
-``/root/reference``; override with ``CUGAL_REFERENCE``)::
+Run where the cuGAL reference is checked out (``CUGAL_REFERENCE``; default: a
+directory ``reference`` beside this repository)::
 
     python tests/golden/make_golden.py
 
@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 HERE = Path(__file__).resolve().parent
-REF = os.environ.get("CUGAL_REFERENCE", "/root/reference")
+REF = os.environ.get("CUGAL_REFERENCE") or str(HERE.parent.parent.parent / "reference")
 
 
 def import_reference():

@@ -16,7 +16,7 @@ import networkx as nx
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("CUGAL_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("CUGAL_REFERENCE") or Path(__file__).resolve().parents[3] / "reference")
 NAMES = ["edge_correctness", "induced_conserved_structure", "symmetric_substructure", "alignment_accuracy"]
 
 

@@ -13,7 +13,7 @@ import os
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("CUGAL_REFERENCE", "/root/reference")) / "benchmark" / "results"
+REF = Path(os.environ.get("CUGAL_REFERENCE") or Path(__file__).resolve().parents[3] / "reference") / "benchmark" / "results"
 FILES = ["CUGAL_res.json", "FUGAL_res2.json"]
 
 

@@ -88,3 +88,21 @@ def test_exact_lap_reports_nan_and_step_cap():
     P[3, 7] = np.nan
     _, _, status = _ours(P)
     assert status == 5  # FUGAL_NONFINITE
+
+
+def test_rounding_raises_when_the_search_exceeds_its_bound(monkeypatch):
+    """The SCIPY rounding has no host fallback: a search that reaches its step
+    bound (here forced down to 5 steps) is an error, not a silent scipy call."""
+    import cugal_b200.exact_lap as EL
+    from cugal_b200 import _native as N
+    from cugal_b200.config import Config, HungarianMethod
+    from cugal_b200.pred import round_on_device
+    from cugal_b200.profile import Profile
+    P = torch.tensor(np.random.default_rng(2).random((64, 64)).astype(np.float32), device="cuda")
+    cfg = Config(device="cuda", dtype=torch.float32, hungarian_method=HungarianMethod.SCIPY)
+    _, cols = round_on_device(P, cfg, Profile())
+    np.testing.assert_array_equal(np.asarray(cols.cpu() if isinstance(cols, torch.Tensor) else cols),
+                                  _scipy(P.cpu().numpy()))
+    monkeypatch.setattr(EL, "default_max_steps", lambda n: 5)
+    with pytest.raises(N.NativeError, match="Dijkstra steps"):
+        round_on_device(P, cfg, Profile())

@@ -387,3 +387,40 @@ def test_full_alignment_matches_oracle(lap):
     assert abs(prof.sparsity - sp32) < 0.02
     from cugal_b200 import Phase
     assert set(prof.phase_times) == set(Phase)
+
+
+@pytest.mark.parametrize("threshold", [1e30, "mid"])
+def test_frank_wolfe_threshold_early_stop(threshold):
+    """frank_wolfe_threshold (cugal/pred.py:144): the lambda step's inner loop ends
+    at the first Frank-Wolfe step whose duality gap is below the threshold; the
+    steps taken and the plan match the oracle's."""
+    from cugal_b200 import Config, HungarianMethod, Profile, SinkhornMethod, cugal
+    n = 60
+    g, h, perm = _pair(n, 7)
+    params = dict(sinkhorn_regularization=0.05, sinkhorn_iterations=200, sinkhorn_threshold=1e-5,
+                  sinkhorn_eval_freq=10, mu=1.0, iter_count=3, frank_wolfe_iter_count=10)
+    oracle_kw = dict(sinkhorn_method="LOG", use_sparse_adjacency=True, hungarian_method="DOUBLE_GREEDY", **params)
+    if threshold == "mid":
+        # a threshold between the gaps of the full run: some lambda steps stop early, others do not
+        full = O.FWTrace()
+        O.cugal(nx.Graph(g), nx.Graph(h), O.OracleParams(**oracle_kw), features="cuda", trace=full)
+        gaps = np.sort(np.array(full.gaps))
+        # the widest ratio between neighbouring gaps in the middle half, so that FP32
+        # rounding of the gaps cannot move a decision
+        lo, hi = len(gaps) // 4, 3 * len(gaps) // 4
+        k = lo + int(np.argmax(gaps[lo + 1:hi + 1] / gaps[lo:hi]))
+        threshold = float(np.sqrt(gaps[k] * gaps[k + 1]))
+    cfg = Config(device="cuda", dtype=torch.float32, sinkhorn_method=SinkhornMethod.LOG, use_sparse_adjacency=True,
+                 hungarian_method=HungarianMethod.DOUBLE_GREEDY, frank_wolfe_threshold=threshold, **params)
+    prof = Profile()
+    P, mapping = cugal(nx.Graph(g), nx.Graph(h), cfg, prof)
+    trace = O.FWTrace()
+    Pr, mref, _ = O.cugal(nx.Graph(g), nx.Graph(h), O.OracleParams(frank_wolfe_threshold=threshold, **oracle_kw),
+                          features="cuda", trace=trace)
+    assert prof.frank_wolfe_iterations == trace.frank_wolfe_iterations
+    if threshold == 1e30:
+        assert trace.frank_wolfe_iterations == params["iter_count"]  # one step per lambda
+    else:
+        assert params["iter_count"] < trace.frank_wolfe_iterations < 30
+    assert [m[1] for m in mapping] == [m[1] for m in mref]
+    np.testing.assert_allclose(P, Pr, atol=2e-3)

@@ -50,6 +50,30 @@ def test_csr_and_features_bit_exact(name):
         assert np.array_equal(avg, O.average_neighbor(rp, col, vals.cpu().numpy()))
 
 
+@pytest.mark.parametrize("workload", ["ba8192", "er32768"])
+def test_workload_degrees_and_triangles_bit_exact(workload):
+    """Degrees, triangle counts, clustering and neighbour averages of both graphs
+    of the Barabasi-Albert n=8192 (m=5, seed 1, 5% noise) and Erdos-Renyi
+    n=32768 (mean degree 16, seed 2, 2% noise) workloads, bit for bit."""
+    from cugal_b200.adjacency import Adjacency
+    from cugal_b200.feature_extraction import average_neighbor_features, graph_features
+    from cugal_b200.synthetic import make_pair
+    src, tgt, _, _ = make_pair(workload)
+    for g in (src, tgt):
+        rp, col = O.csr_from_graph(g)
+        A = Adjacency.from_graph(g, "cuda")
+        assert np.array_equal(A.row_pointers.cpu().numpy(), rp)
+        assert np.array_equal(A.col_indices.cpu().numpy(), col)
+        deg, clust, dc, tc = graph_features(A, with_counts=True)
+        odeg, otri = O.triangle_counts(rp, col)
+        assert np.array_equal(dc.cpu().numpy(), odeg)
+        assert np.array_equal(tc.cpu().numpy(), otri)
+        assert np.array_equal(clust.cpu().numpy(), O.clustering_from_counts(odeg, otri))
+        for vals in (deg, clust):
+            avg = average_neighbor_features(A, vals).cpu().numpy()
+            assert np.array_equal(avg, O.average_neighbor(rp, col, vals.cpu().numpy()))
+
+
 def test_features_match_reference_nx_path_within_fp32():
     from cugal_b200.config import Config
     from cugal_b200.feature_extraction import extract_features_cuda
@@ -140,3 +164,30 @@ def test_count_le_matches_numpy():
     eps = float(torch.finfo(torch.float32).eps)
     N.call("fugal_count_le", P.data_ptr(), 333, 333, eps, cnt.data_ptr(), N.stream_handle())
     assert int(cnt.item()) == int((P.cpu().numpy() <= eps).sum())
+
+
+@pytest.mark.parametrize("n,case", [(300, "plain"), (300, "zeros"), (1000, "plain"), (70, "ties")])
+def test_more_rand_rounding_matches_oracle(n, case):
+    """MORE_RAND (cugal/greedy_lap.py:34-48) with given row order and draws: the
+    same columns and the same mutated P as the oracle."""
+    from cugal_b200.greedy_lap import sampled_assign
+    P = _lap_matrix(n, 9, zero_rows=n // 10 if case == "zeros" else 0, ties=case == "ties")
+    rng = np.random.default_rng(4)
+    order = rng.permutation(n)
+    uniforms = rng.random(n)
+    Pg = torch.tensor(P, device="cuda")
+    cols = sampled_assign(Pg, torch.tensor(order), uniforms).cpu().numpy()
+    Po = P.astype(np.float64)
+    ref = O.greedy_lap(Po, "MORE_RAND", order=order, uniforms=uniforms)
+    assert np.array_equal(cols, ref)
+    assert np.array_equal(Pg.cpu().numpy(), Po.astype(np.float32))
+
+
+def test_more_rand_against_reference_golden():
+    from pathlib import Path
+    from cugal_b200.greedy_lap import sampled_assign
+    g = dict(np.load(Path(__file__).resolve().parent / "golden" / "reference_golden.npz"))
+    Pg = torch.tensor(g["lap_P"], dtype=torch.float32, device="cuda")
+    cols = sampled_assign(Pg, torch.tensor(g["lap_MORE_RAND_order"]), g["lap_MORE_RAND_uniforms"]).cpu().numpy()
+    assert np.array_equal(cols, g["lap_MORE_RAND_cols"])
+    np.testing.assert_allclose(Pg.cpu().numpy(), g["lap_MORE_RAND_P"], rtol=1e-6, atol=0)
