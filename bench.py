@@ -470,8 +470,9 @@ def run_ours(args):
     # time of every launch of the family (the few that return at once included) over the sweeps that ran
     achieved = bytes_per * real / (ms / 1e3) / 1e9 if real else None
     traffic = traffic_per_launch(n, ld) if sdt is not None else None
-    # the row-owned kernel runs 512 threads per CTA without clusters; the cluster sweep at most 256
-    row_owned = sdt is not None and plan.get("threads") == 512 and plan.get("cluster") == 1
+    # the row-owned kernel runs 512 threads per CTA (one CTA, or a two-CTA cluster, per row
+    # block); the cluster sweep at most 256
+    row_owned = sdt is not None and plan.get("threads") == 512
     kernel_name = f"{'row_sweep_kernel' if row_owned else 'sweep_kernel'}<{args.stream_dtype}>"
 
     solves = config.iter_count * config.frank_wolfe_iter_count

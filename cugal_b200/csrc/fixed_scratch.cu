@@ -42,7 +42,10 @@ std::mutex setup_lock;
 void* scratch_address[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device, looked up once per
-// device (the lookup loads this library's device code on that device).
+// device (the lookup loads this library's device code on that device).  The
+// address belongs to the runtime's primary context of that device; a device
+// reset or a different driver context would make it stale (documented as
+// unsupported for this entry point).
 fugal_status scratch_for_current_device(void** out) {
     int dev = -1;
     FUGAL_TRY(cuda_check(cudaGetDevice(&dev), "fugal_fw_gradient_fixed_scratch: cudaGetDevice"));

@@ -251,6 +251,38 @@ template <> struct Pairs<__half> {
 
 FUGAL_DEVICE float2 ex2_pair(float2 x) { return make_float2(ex2(x.x), ex2(x.y)); }
 
+// 2^x for two lanes on the FMA pipe instead of MUFU (Cody-Waite style
+// reduction): k = round(x) by the 1.5 * 2^23 rounding constant, f = x - k in
+// [-1/2, 1/2], 2^f by a degree-6 polynomial, and k added to the result's
+// exponent bits.  The coefficients were fitted for this file by Lawson's
+// iteratively reweighted least squares, minimising the relative error on
+// [-1/2, 1/2]: 1.9e-9 in exact arithmetic, under 8e-8 (about 1 ulp) with FP32
+// Horner steps -- no worse than ex2.approx.  x is clamped to [-127, 127] (so a
+// huge x still gives a huge finite value) and x < -126 gives 0, as
+// ex2.approx.ftz flushes results below 2^-126; -inf gives 0.
+FUGAL_DEVICE float2 ex2_poly_pair(float2 x) {
+    const float2 xc = make_float2(fminf(fmaxf(x.x, -127.f), 127.f), fminf(fmaxf(x.y, -127.f), 127.f));
+    const float2 rnd = make_float2(12582912.f, 12582912.f);  // 1.5 * 2^23
+    const float2 t = __fadd2_rn(xc, rnd);                     // rnd + round(x)
+    const float2 k = __fadd2_rn(t, make_float2(-12582912.f, -12582912.f));
+    const float2 f = __ffma2_rn(k, make_float2(-1.f, -1.f), xc);  // x - k, exact
+    float2 q = make_float2(1.534581242594868e-4f, 1.534581242594868e-4f);
+    q = __ffma2_rn(q, f, make_float2(1.3399930903688073e-3f, 1.3399930903688073e-3f));
+    q = __ffma2_rn(q, f, make_float2(9.618489071726799e-3f, 9.618489071726799e-3f));
+    q = __ffma2_rn(q, f, make_float2(5.550328642129898e-2f, 5.550328642129898e-2f));
+    q = __ffma2_rn(q, f, make_float2(2.4022646248340607e-1f, 2.4022646248340607e-1f));
+    q = __ffma2_rn(q, f, make_float2(6.931471824645996e-1f, 6.931471824645996e-1f));
+    q = __ffma2_rn(q, f, make_float2(1.f, 1.f));
+    // the bits of t are those of rnd plus round(x); rnd's low 9 bits are 0, so
+    // (bits(t) << 23) is round(x) << 23 modulo 2^32: round(x) added to the exponent
+    float2 y;
+    y.x = __int_as_float(__float_as_int(q.x) + (__float_as_int(t.x) << 23));
+    y.y = __int_as_float(__float_as_int(q.y) + (__float_as_int(t.y) << 23));
+    if (x.x < -126.f) y.x = 0.f;
+    if (x.y < -126.f) y.y = 0.f;
+    return y;
+}
+
 // Sweep kernel.  Each thread owns KPT columns of its CTA's slice as KPT/2
 // float pairs and processes R rows per batch; the hot loop runs on Blackwell's
 // packed FP32x2 FMA/ADD (fma.rn.f32x2) with the exponentials on MUFU ex2, in
@@ -672,7 +704,21 @@ __device__ __forceinline__ float sum16(const float* r) {
            (((c.x + c.y) + (c.z + c.w)) + ((d.x + d.y) + (d.z + d.w)));
 }
 
-template <typename T, int EPT, int THREADS, bool BT>
+// POLY: on the fast path, one exponential pair in every POLY (of the 8 pairs of
+// two 8-column chunks) is evaluated on the FMA pipe (ex2_poly_pair) instead of
+// MUFU; 0: none.
+// CL = 2 (rows wider than one CTA covers, up to 65536 columns): a cluster of two
+// CTAs owns each block of rows, CTA k taking columns [k COVER, (k + 1) COVER).
+// After each CTA barrier the two CTAs swap their row partial (sum, or maximum
+// on the exact path) through distributed shared memory: thread 0 stores it
+// into the peer's slot with st.async, completing 8 transaction bytes on the
+// peer's slot barrier, and every thread waits (bounded) on its own slot
+// barrier.  Both CTAs combine the two values in rank order, so they hold the
+// bit-identical row normaliser.  Two slots alternate; a peer reuses a slot only
+// after it has received the next exchange, which this CTA sends after a barrier
+// that follows every read of the slot.  A timed-out exchange is carried to the
+// next barrier vote.
+template <typename T, int EPT, int THREADS, bool BT, int POLY, int CL>
 __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) {
     constexpr int kRowThreads = THREADS;
     constexpr int kRowWarps = THREADS / 32;
@@ -686,8 +732,11 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     static_assert(G % 2 == 0, "column duals load from TMEM 16 at a time");
     static_assert(kRowWarps == 16, "sum16 reduces 16 warp partials");
     static_assert(SEG <= kRowSeg, "segment larger than a stage");
+    static_assert(CL == 1 || (CL == 2 && BT), "two-CTA rows keep the column duals in TMEM");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full[kMaxStages];
+    __shared__ uint64_t xbar[2];
+    __shared__ __align__(8) float2 xs[2];
     __shared__ __align__(16) float red_s[2][kRowWarps];
     __shared__ __align__(16) float red_m[2][kRowWarps];
     __shared__ __align__(16) float red_grp[2][4][kRowWarps];
@@ -698,11 +747,14 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = p.n;
-    constexpr int COVER = kRowThreads * EPT;  // columns the threads cover (>= n)
+    constexpr int COVER = kRowThreads * EPT;  // columns the threads cover (CL COVER >= n)
+    const int rank = CL > 1 ? static_cast<int>(cluster_ctarank()) : 0;
+    const int grp = static_cast<int>(blockIdx.x) / CL;  // row block (cluster) index
+    const int col0 = rank * COVER;                       // first column of this CTA
     float* b_s = reinterpret_cast<float*>(smem);
     unsigned char* stage_base = smem + (BT ? 0 : static_cast<size_t>(COVER) * 4);
     const size_t stage_bytes = static_cast<size_t>(SEG) * sizeof(T);
-    const int row_begin = blockIdx.x * p.rows_per_cta;
+    const int row_begin = grp * p.rows_per_cta;
     const int row_end = min(n, row_begin + p.rows_per_cta);
     const int nrows = max(0, row_end - row_begin);
     const int units = nrows * NSEG;
@@ -734,6 +786,8 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         reinterpret_cast<T*>(stage_base)[k] = from_float<T>(0.f);
     if (tid == 0) {
         for (int s = 0; s < p.stages; ++s) mbar_init(&full[s], 1);
+        mbar_init(&xbar[0], 1);
+        mbar_init(&xbar[1], 1);
         fence_mbarrier_init();
     }
     if (warp == 0) {
@@ -743,6 +797,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     tmem_fence_before_sync();
     __syncthreads();
     tmem_fence_after_sync();
+    if constexpr (CL > 1) cluster_sync();  // the peer's slot barriers exist before anything is sent
     const uint32_t tcol = tmem_slot + (static_cast<uint32_t>(32 * (warp & 3)) << 16) +
                           static_cast<uint32_t>((warp >> 2) * EPT);
     // this thread's column duals: element e (segment e / EPS, chunk (e % EPS) / 8) is column
@@ -766,9 +821,10 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     float b = -INFINITY;
-                    if (c + q < n) {
-                        const float bj = b_prev[c + q] - omega * p.logcs[c + q];
-                        if (blockIdx.x == 0) b_out[c + q] = bj;
+                    const int j = col0 + c + q;
+                    if (j < n) {
+                        const float bj = b_prev[j] - omega * p.logcs[j];
+                        if (grp == 0) b_out[j] = bj;
                         b = bj * kLog2e;
                     }
                     bb[8 * h + q] = b;
@@ -783,13 +839,14 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         const int s = u % p.stages;
         const int row = row_begin + u / NSEG;
         const int seg = u % NSEG;
-        const int cols = min(SEG, p.n_copy - seg * SEG);
+        const int cols = min(SEG, p.n_copy - col0 - seg * SEG);
         const uint32_t bytes = cols > 0 ? static_cast<uint32_t>(cols) * sizeof(T) : 0u;
         const uint32_t unmet = (blockIdx.x == 0 && u == p.fault_row * NSEG) ? 16u : 0u;
         mbar_arrive_expect_tx(&full[s], bytes + unmet);
         if (bytes > 0)
             bulk_load(stage_base + s * stage_bytes,
-                      static_cast<const T*>(p.L) + static_cast<size_t>(row) * p.ld + static_cast<size_t>(seg) * SEG,
+                      static_cast<const T*>(p.L) + static_cast<size_t>(row) * p.ld + col0 +
+                          static_cast<size_t>(seg) * SEG,
                       bytes, &full[s]);
     };
     int issued = 0;
@@ -809,6 +866,21 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                 }
             }
         }
+    };
+    // Swap of one row partial with the peer CTA (CL = 2); returns the peer's value.
+    int xuse = 0;
+    bool xok = true;  // every exchange so far completed (voted on at the next barrier)
+    auto swap_with_peer = [&](float v) -> float {
+        const int slot = xuse & 1;
+        const uint32_t parity = static_cast<uint32_t>((xuse >> 1) & 1);
+        ++xuse;
+        if (tid == 0) {
+            mbar_arrive_expect_tx(&xbar[slot], 8u);
+            const uint32_t peer = static_cast<uint32_t>(rank ^ 1);
+            st_async_f32x2(map_to_rank(&xs[slot], peer), v, 0.f, map_to_rank(&xbar[slot], peer));
+        }
+        xok = mbar_wait(&xbar[slot], parity, &st->status, p.suspend_ns, p.wait_limit_ns) && xok;
+        return xs[slot].x;
     };
     auto b2_at = [&](int c, float2* b2) {  // c: a multiple of 8
         const float4 lo = *reinterpret_cast<const float4*>(b_s + (c >> 3) * 4);
@@ -853,7 +925,10 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                     Pairs<T>::unpack(*reinterpret_cast<const uint4*>(stage + cl), v2);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const float2 e = ex2_pair(__ffma2_rn(v2[q], log2e2, b2[4 * gg + q]));
+                        const float2 xq = __ffma2_rn(v2[q], log2e2, b2[4 * gg + q]);
+                        const float2 e = (POLY > 0 && (4 * gg + q) % (POLY > 0 ? POLY : 1) == (POLY > 0 ? POLY : 1) - 1)
+                                             ? ex2_poly_pair(xq)
+                                             : ex2_pair(xq);
                         yy[(sg * EPS + g * 8) / 2 + q] = e;
                         if (q & 1)
                             t2 = __fadd2_rn(t2, e);
@@ -872,7 +947,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     // the per-warp sums and one pass over the TMEM accumulators.  A group with a
     // row outside the fast path's range hands the rest of the sweep to the
     // single-row loop below, which restarts at that group (stages still held).
-    if constexpr (NSEG == 1 && EPT <= 32) {
+    if constexpr (CL == 1 && NSEG == 1 && EPT <= 32) {
         constexpr int RB = 64 / EPT;  // 2 or 4
         if (!exact_only) {
             for (; r < nrows; r += RB) {
@@ -952,11 +1027,15 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             const float2 u2 = __fadd2_rn(s2, t2);
             const float part = warp_sum(u2.x + u2.y);
             if (lane == 0) red_s[par][warp] = part;
-            if (!__syncthreads_and(ok)) {
+            if (!__syncthreads_and(ok && xok)) {
                 alive = false;
                 break;
             }
-            const float S = sum16(red_s[par]);
+            float S = sum16(red_s[par]);
+            if constexpr (CL > 1) {
+                const float Sp = swap_with_peer(S);
+                S = rank == 0 ? S + Sp : Sp + S;
+            }
             fast_ok = S > 1e-30f && S < 1e30f;  // uniform
             if (fast_ok) {
                 release(r);
@@ -966,6 +1045,9 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         }
         if (!fast_ok) {
             // ---- exact path: row maximum, then the exponentials relative to it
+            // (the previous row dual is read before any exchange of this row, so a
+            // peer that writes it later cannot have written it yet)
+            const float a_old = momentum ? p.a[row] : 0.f;
             float mx = -INFINITY;
 #pragma unroll
             for (int sg = 0; sg < NSEG; ++sg) {
@@ -995,13 +1077,14 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             }
             mx = warp_max(mx);
             if (lane == 0) red_m[par][warp] = mx;
-            if (!__syncthreads_and(ok)) {
+            if (!__syncthreads_and(ok && xok)) {
                 alive = false;
                 break;
             }
             float M2 = -INFINITY;
 #pragma unroll
             for (int w = 0; w < kRowWarps; ++w) M2 = fmaxf(M2, red_m[par][w]);
+            if constexpr (CL > 1) M2 = fmaxf(M2, swap_with_peer(M2));
             const float base = (M2 == -INFINITY) ? 0.f : M2;
             const float2 nb = make_float2(-base, -base);
             float2 ss = make_float2(0.f, 0.f);
@@ -1012,15 +1095,21 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             }
             const float part = warp_sum(ss.x + ss.y);
             if (lane == 0) red_s[par][warp] = part;
-            __syncthreads();
+            if (!__syncthreads_and(xok)) {
+                alive = false;
+                break;
+            }
             release(r);
-            const float S = sum16(red_s[par]);
+            float S = sum16(red_s[par]);
+            if constexpr (CL > 1) {
+                const float Sp = swap_with_peer(S);
+                S = rank == 0 ? S + Sp : Sp + S;
+            }
             const float lse = (M2 + log2f(S)) * kLn2;
-            anew = momentum ? (1.f - omega) * p.a[row] - omega * lse : -lse;
+            anew = momentum ? (1.f - omega) * a_old - omega * lse : -lse;
             wr = (M2 == -INFINITY) ? 0.f : ex2(M2 + anew * kLog2e);
-            if (momentum) __syncthreads();  // every thread has read a[row] before it is overwritten
         }
-        if (tid == 0) p.a[row] = anew;
+        if (tid == 0 && rank == 0) p.a[row] = anew;
         // column sums of the row-normalised plan, accumulated in TMEM (one 16-column
         // chunk per load; batching two chunks per wait measured slower)
         const float2 w2 = make_float2(wr, wr);
@@ -1040,7 +1129,8 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
 
     // per-CTA column sums -> partials[cta][col]
     tmem_wait_st();
-    float* prow = p.partials + static_cast<size_t>(blockIdx.x) * p.n_pad;
+    float* prow = p.partials + static_cast<size_t>(grp) * p.n_pad + col0;
+    const int nloc = n - col0;
 #pragma unroll
     for (int k = 0; k < EPT / 16; ++k) {
         float acc[16];
@@ -1050,12 +1140,12 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             const int e = 16 * k + 8 * half;  // element index: segment e / EPS, chunk (e % EPS) / 8
             const int c = (e / EPS) * SEG + (((e % EPS) / 8) * kRowThreads + tid) * 8;
             const float* src = acc + 8 * half;
-            if (c + 8 <= n) {
+            if (c + 8 <= nloc) {
                 *reinterpret_cast<float4*>(prow + c) = make_float4(src[0], src[1], src[2], src[3]);
                 *reinterpret_cast<float4*>(prow + c + 4) = make_float4(src[4], src[5], src[6], src[7]);
             } else {
                 for (int q = 0; q < 8; ++q)
-                    if (c + q < n) prow[c + q] = src[q];
+                    if (c + q < nloc) prow[c + q] = src[q];
             }
         }
     }
@@ -1072,6 +1162,9 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     __syncthreads();
     tmem_fence_after_sync();
     if (warp == 0) tmem_dealloc(tmem_slot, TCOLS);
+    // no CTA leaves while its peer may still send into its shared memory; the
+    // non-aligned form tolerates threads that left the row loop early
+    if constexpr (CL > 1) cluster_sync_any();
 }
 
 // Reduce the per-cluster column sums (FP64), write log(colsum), decide.
@@ -1507,6 +1600,9 @@ fugal_status make_plan(int64_t n, int dt, int kind, SweepPlan& pl, bool query_oc
 struct RowPlan {
     bool use = false;
     bool bt = true;
+    int poly = 0;
+    int cl = 1;      // CTAs per row block (a cluster when 2)
+    int groups = 0;  // row blocks (rows of column partials)
     int threads = 512;
     int ept = 0;
     int ctas = 0;
@@ -1518,16 +1614,35 @@ struct RowPlan {
 
 using RowKernelFn = void (*)(const RowArgs);
 
-template <typename T, bool BT>
-RowKernelFn row_kernel_typed(int ept) {
-    return ept == 16 ? row_sweep_kernel<T, 16, 512, BT>
-                     : (ept == 32 ? row_sweep_kernel<T, 32, 512, BT> : row_sweep_kernel<T, 64, 512, BT>);
+template <typename T, bool BT, int POLY>
+RowKernelFn row_kernel_typed(int ept, int cl) {
+    if (cl == 2) return row_sweep_kernel<T, 64, 512, BT, POLY, (BT ? 2 : 1)>;
+    return ept == 16 ? row_sweep_kernel<T, 16, 512, BT, POLY, 1>
+                     : (ept == 32 ? row_sweep_kernel<T, 32, 512, BT, POLY, 1> : row_sweep_kernel<T, 64, 512, BT, POLY, 1>);
 }
 
-RowKernelFn row_kernel_for(int dt, int ept, int threads, bool bt) {
+template <typename T>
+RowKernelFn row_kernel_dt(int ept, bool bt, int poly, int cl) {
+    if (!bt) return row_kernel_typed<T, false, 0>(ept, 1);
+    switch (poly) {
+        case 4: return row_kernel_typed<T, true, 4>(ept, cl);
+        case 8: return row_kernel_typed<T, true, 8>(ept, cl);
+        default: return row_kernel_typed<T, true, 0>(ept, cl);
+    }
+}
+
+RowKernelFn row_kernel_for(int dt, int ept, int threads, bool bt, int poly, int cl) {
     (void)threads;
-    if (bt) return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16, true>(ept) : row_kernel_typed<__half, true>(ept);
-    return dt == FUGAL_BF16 ? row_kernel_typed<__nv_bfloat16, false>(ept) : row_kernel_typed<__half, false>(ept);
+    return dt == FUGAL_BF16 ? row_kernel_dt<__nv_bfloat16>(ept, bt, poly, cl)
+                            : row_kernel_dt<__half>(ept, bt, poly, cl);
+}
+
+// Share of the row sweep's fast-path exponentials evaluated on the FMA pipe:
+// one pair in FUGAL_ROW_POLY (4 or 8); unset or 0: all on MUFU.
+int row_poly() {
+    const char* e = getenv("FUGAL_ROW_POLY");
+    const int v = e != nullptr ? atoi(e) : 0;
+    return (v == 4 || v == 8) ? v : 0;
 }
 
 // Failure-detection test hooks of the row sweep, read from the environment at
@@ -1560,26 +1675,48 @@ fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool s
     if (dt == FUGAL_F32) return FUGAL_OK;
     const char* e = getenv("FUGAL_ROW_SWEEP");
     if (e != nullptr && atoi(e) == 0) return FUGAL_OK;
-    if (n_pad > 32768) return FUGAL_OK;
+    rp.bt = row_duals_in_tmem();
+    // rows up to 32768 columns: one CTA; up to 65536: a cluster of two (duals in TMEM)
+    if (n_pad > (rp.bt ? 65536 : 32768)) return FUGAL_OK;
     rp.threads = row_threads_for(n_pad);
-    rp.ept = static_cast<int>((n_pad + rp.threads * 16 - 1) / (rp.threads * 16)) * 16;  // 16, 32 or 64
+    rp.cl = n_pad > 32768 ? 2 : 1;
+    const int64_t per_cta = (n_pad + rp.cl - 1) / rp.cl;
+    rp.ept = static_cast<int>((per_cta + rp.threads * 16 - 1) / (rp.threads * 16)) * 16;  // 16, 32 or 64
     if (rp.ept == 48) rp.ept = 64;
     const size_t stage_bytes = static_cast<size_t>(rp.threads) * std::min(rp.ept, kRowSeg / rp.threads) * 2;
-    rp.bt = row_duals_in_tmem();
+    rp.poly = rp.bt ? row_poly() : 0;
     // column duals of every covered column, unless they live in TMEM
     const size_t fixed = rp.bt ? 0 : static_cast<size_t>(rp.threads) * rp.ept * 4;
     const int64_t room = static_cast<int64_t>(max_smem_optin()) - 1024 - static_cast<int64_t>(fixed);
     rp.stages = static_cast<int>(std::min<int64_t>(kMaxStages, room / static_cast<int64_t>(stage_bytes)));
     if (rp.stages < 2) return FUGAL_OK;
     rp.smem = fixed + rp.stages * stage_bytes;
-    const int ctas = static_cast<int>(std::min<int64_t>(sm_count(), n));
-    rp.rows_per_cta = static_cast<int>((n + ctas - 1) / ctas);
-    rp.ctas = static_cast<int>((n + rp.rows_per_cta - 1) / rp.rows_per_cta);
+    int groups = static_cast<int>(std::min<int64_t>(sm_count() / rp.cl, n));
+    RowKernelFn fn = row_kernel_for(dt, rp.ept, rp.threads, rp.bt, rp.poly, rp.cl);
     if (set_attributes) {
-        RowKernelFn fn = row_kernel_for(dt, rp.ept, rp.threads, rp.bt);
         FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp.smem),
                              "sinkhorn: row sweep shared memory"));
+        if (rp.cl > 1) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            cfg.gridDim = dim3(rp.cl, 1, 1);
+            cfg.blockDim = dim3(rp.threads, 1, 1);
+            cfg.dynamicSmemBytes = rp.smem;
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = rp.cl;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int active = 0;
+            FUGAL_TRY(cuda_check(cudaOccupancyMaxActiveClusters(&active, fn, &cfg), "sinkhorn: row cluster occupancy"));
+            if (active <= 0) return FUGAL_OK;  // no two-CTA cluster fits: the cluster sweep takes over
+            groups = static_cast<int>(std::min<int64_t>(active, n));
+        }
     }
+    rp.rows_per_cta = static_cast<int>((n + groups - 1) / groups);
+    rp.groups = static_cast<int>((n + rp.rows_per_cta - 1) / rp.rows_per_cta);
+    rp.ctas = rp.groups * rp.cl;
     rp.use = true;
     return FUGAL_OK;
 }
@@ -1685,8 +1822,8 @@ extern "C" fugal_status fugal_sinkhorn_plan_info(int64_t n, int stream_dtype, in
     FUGAL_TRY(make_row_plan(n, stream_dtype, static_cast<int64_t>(align_up(static_cast<size_t>(n), 64)), rp, false));
     if (rp.use) {  // row-owned sweep: one CTA per SM, no cluster
         info[0] = rp.threads;
-        info[1] = 1;
-        info[2] = rp.ctas;
+        info[1] = rp.cl;
+        info[2] = rp.groups;
         info[3] = rp.stages;
         info[4] = static_cast<int32_t>(rp.smem);
         info[5] = 1;
@@ -1744,7 +1881,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         FUGAL_TRY(make_plan(n, FUGAL_F32, p.stream_dtype == FUGAL_BF16 ? 1 : 2, plan_abs, true));
     }
     if (plan32.clusters > prow || (use16 && (plan16.clusters > prow || plan_abs.clusters > prow)) ||
-        rowplan.ctas > prow)
+        rowplan.groups > prow)
         return fail(FUGAL_UNSUPPORTED, "fugal_sinkhorn_solve: more clusters than partial rows");
 
     FrameArgs frame{use16 ? 1 : 0, use16 ? p.fp32_warmup_sweeps : 0, use16 ? p.reabsorb_every : 1,
@@ -1876,11 +2013,28 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
             ra.fault_row = test_fault_row();
             {
                 LaunchScope scope(FUGAL_KERNEL_SWEEP, stream);
-                row_kernel_for(p.stream_dtype, rowplan.ept, rowplan.threads, rowplan.bt)
-                    <<<rowplan.ctas, rowplan.threads, rowplan.smem, stream>>>(ra);
-                status = launch_check("sinkhorn: row sweep");
+                RowKernelFn fn = row_kernel_for(p.stream_dtype, rowplan.ept, rowplan.threads, rowplan.bt,
+                                                rowplan.poly, rowplan.cl);
+                if (rowplan.cl == 1) {
+                    fn<<<rowplan.ctas, rowplan.threads, rowplan.smem, stream>>>(ra);
+                    status = launch_check("sinkhorn: row sweep");
+                } else {
+                    cudaLaunchConfig_t cfg = {};
+                    cudaLaunchAttribute attr[1];
+                    cfg.gridDim = dim3(rowplan.ctas, 1, 1);
+                    cfg.blockDim = dim3(rowplan.threads, 1, 1);
+                    cfg.dynamicSmemBytes = rowplan.smem;
+                    cfg.stream = stream;
+                    attr[0].id = cudaLaunchAttributeClusterDimension;
+                    attr[0].val.clusterDim.x = rowplan.cl;
+                    attr[0].val.clusterDim.y = 1;
+                    attr[0].val.clusterDim.z = 1;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = 1;
+                    status = cuda_check(cudaLaunchKernelEx(&cfg, fn, ra), "sinkhorn: row sweep launch");
+                }
             }
-            if (status == FUGAL_OK) status = finalize(rowplan.ctas);
+            if (status == FUGAL_OK) status = finalize(rowplan.groups);
         } else {
             SweepArgs a = sweep_args(plan16, p.cost16, p.ld16, nullptr, nullptr);
             status = launch_sweep(plan16, kernel_for(plan16.threads, plan16.kpt, p.stream_dtype, 0), a, stream, FUGAL_KERNEL_SWEEP);

@@ -284,9 +284,12 @@ fugal_status fugal_fw_gradient_column_stats(int64_t n, const int32_t* a_row_poin
  * process exits.  n above FUGAL_FIXED_SCRATCH_MAX_N is rejected with
  * FUGAL_BAD_SHAPE.  The call allocates nothing.  Its first call on a device (that
  * device current) looks up the array's device address; make that first call
- * before any stream capture.  All calls on a device share the array and it keeps
- * the last call's contents (nothing in it needs to start at zero); calls whose
- * kernels overlap on the GPU race on it, so order them on one stream. */
+ * before any stream capture.  The address is kept per device for the runtime's
+ * primary context: after a cudaDeviceReset, or from another driver context, the
+ * kept address is stale, so such callers must not use this entry point.  All
+ * calls on a device share the array and it keeps the last call's contents
+ * (nothing in it needs to start at zero); calls whose kernels overlap on the GPU
+ * race on it, so order them on one stream. */
 #define FUGAL_FIXED_SCRATCH_BYTES (16 * 1024 * 1024)
 #define FUGAL_FIXED_SCRATCH_MAX_N 2048
 fugal_status fugal_fw_gradient_fixed_scratch(int64_t n, const int32_t* a_row_pointers,

@@ -232,3 +232,30 @@ def double_greedy(P: torch.Tensor) -> np.ndarray:
         taken[m] = 0
         res[r] = m
     return res
+
+
+def solve_log_differentiable(C: torch.Tensor, reg: float, iterations: int, segment: int = 25) -> torch.Tensor:
+    """The reference's ``solve_log`` (``cugal/sinkhorn.py:99-116``, no momentum,
+    zero start) as plain differentiable torch ops for ``iterations`` iterations:
+    K = -C/reg; v = -LSE_i(K + u), u = -LSE_j(K + v); returns P = exp(K + u + v).
+    Autograd through it is torch autograd through the reference's iteration;
+    the iterations are recomputed segment by segment on the way back
+    (``torch.utils.checkpoint``) so the memory held is one segment's."""
+    import torch.utils.checkpoint as ckpt
+    K = -C / reg
+    n = C.shape[0]
+    u = torch.zeros(n, dtype=C.dtype, device=C.device)
+    v = torch.zeros(n, dtype=C.dtype, device=C.device)
+
+    def run(K, u, v, k):
+        for _ in range(k):
+            v = -torch.logsumexp(K + u[:, None], dim=0)
+            u = -torch.logsumexp(K + v[None, :], dim=1)
+        return u, v
+
+    done = 0
+    while done < iterations:
+        k = min(segment, iterations - done)
+        u, v = ckpt.checkpoint(run, K, u, v, k, use_reentrant=False)
+        done += k
+    return torch.exp(K + u[:, None] + v[None, :])

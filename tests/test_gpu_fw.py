@@ -222,7 +222,7 @@ def test_sinkhorn_reduced_precision_stream(dtype, tol, n, kernel, monkeypatch):
     np.testing.assert_allclose(P.sum(axis=1), 1.0, atol=1e-4)  # rows exact after the FP32 polish sweep
 
 
-def _solve_device(Ct, reg, max_iter, stream_dtype=None, polish=1, warmup=3, every=4):
+def _solve_device(Ct, reg, max_iter, stream_dtype=None, polish=1, warmup=3, every=4, mstart=None):
     """Zero-start solve of the device cost Ct (n x n FP32, torch): (u, v) FP64 numpy."""
     from cugal_b200 import _native as N
     from cugal_b200.config import Config, SinkhornMethod
@@ -231,7 +231,7 @@ def _solve_device(Ct, reg, max_iter, stream_dtype=None, polish=1, warmup=3, ever
     cfg = Config(device="cuda", dtype=torch.float32, sinkhorn_method=SinkhornMethod.LOG,
                  sinkhorn_regularization=reg, sinkhorn_iterations=max_iter, sinkhorn_threshold=0.0,
                  sinkhorn_eval_freq=10, stream_dtype=stream_dtype, polish_sweeps=polish, fp32_warmup_sweeps=warmup,
-                 reabsorb_every=every)
+                 reabsorb_every=every, sinkhorn_momentum_start=mstart)
     solver = SinkhornSolver(n, cfg, "cuda")
     cost = torch.zeros((n, padded_ld(n)), dtype=torch.float32, device="cuda")
     cost[:, :n] = Ct / -reg
@@ -243,17 +243,24 @@ def _solve_device(Ct, reg, max_iter, stream_dtype=None, polish=1, warmup=3, ever
     return du.cpu().numpy().astype(np.float64), dv.cpu().numpy().astype(np.float64)
 
 
-@pytest.mark.parametrize("n", [17000, 20000, 32768])
-def test_row_sweep_matches_cluster_sweep_and_fp32(n, monkeypatch):
-    """16-bit solves with the row-owned sweep (two row segments, padded columns)
-    against the cluster sweep and the FP32 stream on the same problem."""
+@pytest.mark.parametrize("n,mstart", [(17000, None), (20000, None), (32768, None), (40000, None), (65536, None),
+                                      (40000, 4)])
+def test_row_sweep_matches_cluster_sweep_and_fp32(n, mstart, monkeypatch):
+    """16-bit solves with the row-owned sweep (two row segments, padded columns;
+    above 32768 columns a two-CTA cluster per row block, with momentum on the
+    exact path in one case) against the cluster sweep and the FP32 stream on the
+    same problem."""
+    from cugal_b200 import _native as N
+    plan = N.sinkhorn_plan(n, N.FUGAL_BF16)
+    assert plan["threads"] == 512 and plan["cluster"] == (2 if n > 32768 else 1), plan
     g = torch.Generator(device="cuda").manual_seed(n)
     Ct = torch.rand((n, n), generator=g, device="cuda") * 4
     reg = 0.05
-    u_r, v_r = _solve_device(Ct, reg, 12, stream_dtype=torch.bfloat16)
+    kw = dict(mstart=mstart) if mstart else {}
+    u_r, v_r = _solve_device(Ct, reg, 12, stream_dtype=torch.bfloat16, **kw)
     monkeypatch.setenv("FUGAL_ROW_SWEEP", "0")
-    u_c, v_c = _solve_device(Ct, reg, 12, stream_dtype=torch.bfloat16)
-    u_f, v_f = _solve_device(Ct, reg, 12)
+    u_c, v_c = _solve_device(Ct, reg, 12, stream_dtype=torch.bfloat16, **kw)
+    u_f, v_f = _solve_device(Ct, reg, 12, **kw)
     rows = np.random.default_rng(n).choice(n, 64, replace=False)
     Cs = Ct[torch.tensor(rows, device="cuda")].double().cpu().numpy()
     del Ct

@@ -74,6 +74,17 @@ def test_fixed_scratch_gradient_matches_workspace_gradient_twice_in_a_row():
     torch.testing.assert_close(got, expect, rtol=1e-5, atol=1e-5 * expect.abs().max().item())
 
 
+@pytest.mark.gpu
+def test_fixed_scratch_gradient_at_its_size_limit():
+    """n = FUGAL_FIXED_SCRATCH_MAX_N, a multiple of 4: the intermediate fills the
+    scratch array exactly."""
+    x = _inputs(MAX_N, 13, with_features=True, with_duals=True)
+    assert MAX_N * ((MAX_N + 3) // 4 * 4) * 4 == 16 * 1024 * 1024
+    got, expect = _both(x, lam=1.5, out_scale=-1.0)
+    assert torch.isfinite(got).all()
+    torch.testing.assert_close(got, expect, rtol=1e-5, atol=1e-5 * expect.abs().max().item())
+
+
 def test_fixed_scratch_rejects_sizes_above_its_limit():
     with pytest.raises(N.NativeError, match="fixed scratch limit"):
         N.call("fugal_fw_gradient_fixed_scratch", MAX_N + 1, *([None] * 5), MAX_N + 1, None, None, None, 0,
