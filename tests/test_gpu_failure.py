@@ -54,3 +54,26 @@ def test_row_sweep_wait_timeout_is_reported_and_context_survives(monkeypatch):
     assert [m[1] for m in map2] == [m[1] for m in map_ok]
     np.testing.assert_array_equal(P2, P_ok)
     assert os.environ.get("FUGAL_TEST_FAULT_ROW") is None
+
+
+def test_safe_mode_rejects_nonfinite_features():
+    """Host-injected fault: a NaN feature weight with safe_mode set stops the
+    alignment with the reference's assertion (cugal/pred.py:222-224)."""
+    from cugal_b200 import Profile, cugal
+    from cugal_b200.config import Config, SinkhornMethod
+    g = nx.newman_watts_strogatz_graph(64, 6, 0.1, seed=3)
+    cfg = Config(device="cuda", dtype=torch.float32, sinkhorn_method=SinkhornMethod.LOG, mu=float("nan"),
+                 safe_mode=True, iter_count=1, frank_wolfe_iter_count=1)
+    with pytest.raises(AssertionError, match="NaN"):
+        cugal(nx.Graph(g), nx.Graph(g), cfg, Profile())
+
+
+def test_mismatched_sizes_are_rejected_before_any_launch():
+    from cugal_b200.adjacency import Adjacency
+    from cugal_b200.config import Config, SinkhornMethod
+    from cugal_b200.pred import FrankWolfeEngine
+    A = Adjacency.from_graph(nx.path_graph(30), "cuda")
+    B = Adjacency.from_graph(nx.path_graph(31), "cuda")
+    cfg = Config(device="cuda", dtype=torch.float32, sinkhorn_method=SinkhornMethod.LOG)
+    with pytest.raises(ValueError, match="same number of nodes"):
+        FrankWolfeEngine(A, B, torch.zeros((30, 30), device="cuda"), cfg)
