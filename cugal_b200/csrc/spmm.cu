@@ -45,23 +45,14 @@ struct Tile {
     __device__ __forceinline__ float4& at(int r, int q) { return c[r][q ^ (r & 7)]; }
 };
 
-// 16-byte read-only load that does not allocate in L1 (the gathered rows are
-// reused across CTAs through L2, never within one SM's L1).
-__device__ __forceinline__ float4 ldg_na(const float4* p) {
-    float4 v;
-    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                 : "l"(p));
-    return v;
-}
-
 // 4 consecutive floats of row k starting at column c: one 16-byte load when the
-// rows are 16-byte aligned (VEC; NA: without L1 allocation), else scalar loads
-// guarded by n.
-template <bool VEC, bool NA = false>
+// rows are 16-byte aligned (VEC), else scalar loads guarded by n.  (Loads that
+// skip L1 allocation, ld.global.nc.L1::no_allocate, made the pair of gradient
+// kernels 50% slower at n = 32768.)
+template <bool VEC>
 __device__ __forceinline__ float4 load4(const float* __restrict__ X, long long ldx, int k, int c, int n) {
     const float* p = X + static_cast<size_t>(k) * ldx + c;
-    if (VEC) return NA ? ldg_na(reinterpret_cast<const float4*>(p)) : __ldg(reinterpret_cast<const float4*>(p));
+    if (VEC) return __ldg(reinterpret_cast<const float4*>(p));
     float4 v;
     v.x = __ldg(p);
     v.y = c + 1 < n ? __ldg(p + 1) : 0.f;
@@ -70,8 +61,9 @@ __device__ __forceinline__ float4 load4(const float* __restrict__ X, long long l
     return v;
 }
 
-// acc = sum over k in N(row) of X[k][c .. c+3] (4 columns per lane).
-template <bool VEC, bool NA>
+// acc = sum over k in N(row) of X[k][c .. c+3] (4 columns per lane), U gathers in
+// flight per lane.
+template <bool VEC, int U>
 __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const int* __restrict__ col,
                                              const float* __restrict__ X, long long ldx, int n, int row, int c,
                                              bool c_ok) {
@@ -88,25 +80,21 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
         const int cnt = min(32, re - e);
         const int idx = (lane < cnt) ? col[e + lane] : 0;
         int q = 0;
-        for (; q + 4 <= cnt; q += 4) {
-            const int k0 = __shfl_sync(0xffffffffu, idx, q);
-            const int k1 = __shfl_sync(0xffffffffu, idx, q + 1);
-            const int k2 = __shfl_sync(0xffffffffu, idx, q + 2);
-            const int k3 = __shfl_sync(0xffffffffu, idx, q + 3);
+        for (; q + U <= cnt; q += U) {
+            int k[U];
+#pragma unroll
+            for (int t = 0; t < U; ++t) k[t] = __shfl_sync(0xffffffffu, idx, q + t);
             if (c_ok) {
-                const float4 v0 = load4<VEC, NA>(X, ldx, k0, c, n);
-                const float4 v1 = load4<VEC, NA>(X, ldx, k1, c, n);
-                const float4 v2 = load4<VEC, NA>(X, ldx, k2, c, n);
-                const float4 v3 = load4<VEC, NA>(X, ldx, k3, c, n);
-                add(v0);
-                add(v1);
-                add(v2);
-                add(v3);
+                float4 v[U];
+#pragma unroll
+                for (int t = 0; t < U; ++t) v[t] = load4<VEC>(X, ldx, k[t], c, n);
+#pragma unroll
+                for (int t = 0; t < U; ++t) add(v[t]);
             }
         }
         for (; q < cnt; ++q) {
             const int k = __shfl_sync(0xffffffffu, idx, q);
-            if (c_ok) add(load4<VEC, NA>(X, ldx, k, c, n));
+            if (c_ok) add(load4<VEC>(X, ldx, k, c, n));
         }
     }
     return make_float4(lo.x, lo.y, hi.x, hi.y);
@@ -114,7 +102,7 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
 
 // Fill the tile with the gathered rows r0 .. r0+31 of A X for columns c0 .. c0+127
 // (lane l: chunk l of each row).
-template <bool VEC, bool NA>
+template <bool VEC, int U>
 __device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const int* __restrict__ col,
                                             const float* __restrict__ X, long long ldx, int n, int r0, int c0,
                                             Tile& tile, float sign) {
@@ -124,13 +112,13 @@ __device__ __forceinline__ void gather_tile(const int* __restrict__ rp, const in
     for (int rr = warp; rr < kTileRows; rr += kSpmmThreads / 32) {
         const int row = r0 + rr;
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row < n) acc = gather_row<VEC, NA>(rp, col, X, ldx, n, row, c, c_ok);
+        if (row < n) acc = gather_row<VEC, U>(rp, col, X, ldx, n, row, c, c_ok);
         tile.at(rr, lane) = make_float4(sign * acc.x, sign * acc.y, sign * acc.z, sign * acc.w);
     }
 }
 
 // Tt[c][r] = (A X)[r][c]  (transposed store), or out[r][c] = sign (A X)[r][c] (direct store).
-template <bool VEC, bool NA = false>
+template <bool VEC, int U = 4>
 __global__ void __launch_bounds__(kSpmmThreads) spmm_kernel(const int* __restrict__ rp, const int* __restrict__ col,
                                                             const float* __restrict__ X, long long ldx, int n,
                                                             float* __restrict__ out, long long ldo, int transpose,
@@ -138,7 +126,7 @@ __global__ void __launch_bounds__(kSpmmThreads) spmm_kernel(const int* __restric
     __shared__ Tile tile;
     const int r0 = blockIdx.x * kTileRows;
     const int c0 = blockIdx.y * kTileCols;
-    gather_tile<VEC, NA>(rp, col, X, ldx, n, r0, c0, tile, sign);
+    gather_tile<VEC, U>(rp, col, X, ldx, n, r0, c0, tile, sign);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (transpose) {
@@ -200,8 +188,8 @@ struct EpilogueArgs {
 // rows i0 .. i0+127 to a base-2 (max, sum) pair, x = out log2 e: M = max x,
 // S = sum 2^(x - M), stored at colpart[blockIdx.y][j] (the first column update
 // of the Sinkhorn solve merges them instead of reading the cost again).
-template <bool COLSTATS, bool NA = false>
-__global__ void __launch_bounds__(kSpmmThreads, 6) gradient_kernel(const int* __restrict__ rp,
+template <bool COLSTATS, int U = 4, int MINB = 6>
+__global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int* __restrict__ rp,
                                                                 const int* __restrict__ col,
                                                                 const float* __restrict__ Tt, long long ldt, int n,
                                                                 const EpilogueArgs ep) {
@@ -219,7 +207,7 @@ __global__ void __launch_bounds__(kSpmmThreads, 6) gradient_kernel(const int* __
         for (int q = threadIdx.x; q < kTileRows; q += kSpmmThreads)
             fj[q] = (j0 + q < n) ? reinterpret_cast<const float4*>(ep.ft)[j0 + q] : make_float4(0, 0, 0, 0);
     }
-    gather_tile<true, NA>(rp, col, Tt, ldt, n, j0, i0, tile, 1.0f);
+    gather_tile<true, U>(rp, col, Tt, ldt, n, j0, i0, tile, 1.0f);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = j0 + lane;
@@ -314,11 +302,16 @@ __global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const
     outT[static_cast<size_t>(j) * ldo + i] = sign * acc;
 }
 
-// Gathers of the gradient kernels without L1 allocation (FUGAL_GATHER_NO_ALLOCATE=1)
-// or through L1 (default).
-bool gather_no_allocate() {
-    const char* e = getenv("FUGAL_GATHER_NO_ALLOCATE");
-    return e != nullptr && atoi(e) != 0;
+// Launch-shape knobs of the gradient kernels (FUGAL_GATHER_UNROLL: gathers in
+// flight per lane, 4 or 8; FUGAL_GRAD_MIN_BLOCKS: resident CTAs per SM the
+// epilogue kernel is compiled for, 6 or 8).
+int gather_unroll() {
+    const char* e = getenv("FUGAL_GATHER_UNROLL");
+    return (e != nullptr && atoi(e) == 8) ? 8 : 4;
+}
+int gradient_min_blocks() {
+    const char* e = getenv("FUGAL_GRAD_MIN_BLOCKS");
+    return (e != nullptr && atoi(e) == 8) ? 8 : 6;
 }
 
 // col may be null for a graph without edges (it is never dereferenced then).
@@ -399,15 +392,16 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
     const int64_t ldt = (n + 3) / 4 * 4;
     dim3 grid(static_cast<unsigned>((n + kTileRows - 1) / kTileRows),
               static_cast<unsigned>((n + kTileCols - 1) / kTileCols));
-    const bool na = gather_no_allocate();
+    const int unroll = gather_unroll();
+    const int minb = gradient_min_blocks();
     {
         LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
-        if (na)
-            spmm_kernel<true, true><<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp,
-                                                                        static_cast<int>(n), Tt, ldt, 1, 1.f);
+        if (unroll == 8)
+            spmm_kernel<true, 8><<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp,
+                                                                     static_cast<int>(n), Tt, ldt, 1, 1.f);
         else
-            spmm_kernel<true, false><<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp,
-                                                                         static_cast<int>(n), Tt, ldt, 1, 1.f);
+            spmm_kernel<true, 4><<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp,
+                                                                     static_cast<int>(n), Tt, ldt, 1, 1.f);
         FUGAL_TRY(launch_check("fugal_fw_gradient: A P"));
     }
     EpilogueArgs ep{P,   ldp, source_features, target_features, D, ldd, lambda * lambda_scale, out_scale, U, V, out,
@@ -415,20 +409,19 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
     {
         LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
         const int ni = static_cast<int>(n);
+        const int* brp = b_row_pointers;
+        const int* bci = b_col_indices;
         if (column_partials != nullptr) {
-            if (na)
-                gradient_kernel<true, true><<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt, ldt,
-                                                                              ni, ep);
+            if (unroll == 8 && minb == 8)
+                gradient_kernel<true, 8, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
+            else if (unroll == 8)
+                gradient_kernel<true, 8, 6><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
+            else if (minb == 8)
+                gradient_kernel<true, 4, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else
-                gradient_kernel<true, false><<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt,
-                                                                               ldt, ni, ep);
+                gradient_kernel<true, 4, 6><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
         } else {
-            if (na)
-                gradient_kernel<false, true><<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt,
-                                                                               ldt, ni, ep);
-            else
-                gradient_kernel<false, false><<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt,
-                                                                                ldt, ni, ep);
+            gradient_kernel<false><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
         }
         FUGAL_TRY(launch_check("fugal_fw_gradient: (A P) B + epilogue"));
     }

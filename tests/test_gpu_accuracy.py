@@ -80,8 +80,15 @@ def test_nws1000_against_reference_fp64(variant, stream):
           f"objective {obj:.6f} vs {obj_ref:.6f} (rel {abs(obj - obj_ref) / abs(obj_ref):.2e}); "
           f"max|P-P64| {perr:.3e}; same column {same_map:.4f}; mean sweeps {sweeps.mean():.2f} vs "
           f"{g[pre + 'sk_iters'].mean():.2f}")
-    assert abs(acc - float(g[pre + "accuracy"])) <= 0.02
-    assert abs(obj - obj_ref) <= 1e-2 * abs(obj_ref)
+    # The lambda schedule drives P to a vertex and the NWS graph has many near-ties, so
+    # rounding-level differences (FP32 or BF16 against FP64, FP32 against FP64 features)
+    # move individual rows to other vertices: max|P - P64| is 1 at those rows.  Measured:
+    # accuracy within 0.3 pt (sparse path) and 0.8 pt (dense path, doubled lambda term),
+    # objective within 1e-2 relative, 88-94% of rows on the reference's column.
+    tol = 0.005 if variant == "sparse" else 0.01
+    assert abs(acc - float(g[pre + "accuracy"])) <= tol
+    assert abs(obj - obj_ref) <= 1.5e-2 * abs(obj_ref)
+    assert same_map >= 0.85
 
 
 def _er32768_pair():
@@ -140,7 +147,12 @@ def test_er32768_first_lambda_block_against_fp64():
               f"{obj64:.6f} (rel {rel:.2e}); sweeps {sweeps} vs FP64 {trace.sinkhorn_iterations}; "
               f"FP64 final errors {['%.1e' % e for e in trace.sinkhorn_final_errors]}")
         del P
-        assert rel <= 1e-2
+        # measured: FP32 max|P - P64| 4.8e-4, BF16 2.2e-2; objective 5e-5 relative for both;
+        # BF16 runs the FP64 solve's iteration counts, FP32 caps one more early solve
+        assert rel <= 2e-4
+        assert err <= (2e-3 if stream == "fp32" else 5e-2)
+        if stream == "bf16":
+            assert sweeps == trace.sinkhorn_iterations
     del P64
     torch.cuda.empty_cache()
 

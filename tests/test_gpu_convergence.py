@@ -1,17 +1,17 @@
-"""Why some Sinkhorn solves run to the 500-iteration cap: the FP32 floor of the
-column-marginal error.
+"""Why some Sinkhorn solves run to the 500-iteration cap: the algorithm, not FP32.
 
 On the Barabasi-Albert n=8192 workload (m 5, seed 1, 5% noise; reg 1e-3,
 tolerance 1e-4 on the L1 column error summed over n columns) the Frank-Wolfe
-engine is run for a few steps; the absorbed cost of the next step (FP32, exactly
+engine is run for five steps; the absorbed cost of the sixth step (FP32, exactly
 as the solve receives it) is then solved twice from the same start: by this
-path (FP32 stream) and by the FP64 restatement of the reference's solve_log
-(oracle/fugal_torch64.py) on the same FP32 values.  The FP64 solve reaches the
-tolerance; the FP32 one cannot, because the L1 error of an FP32-evaluated plan
-does not fall below a floor of about n x (FP32 rounding of a column sum), which
-at n=8192 is above 1e-4 -- the same floor the reference's own FP32 GPU path
-meets.  The plans agree closely once both have converged as far as they can,
-so the extra iterations change the answer only at rounding level."""
+path and by the FP64 restatement of the reference's solve_log
+(oracle/fugal_torch64.py) on the same values.  Both run to the cap with the
+column error near 1e2, far above both the tolerance and the FP32 rounding
+floor of the error (about n 2^-24 = 5e-4): at reg 1e-3 this problem converges
+slowly in any precision (the error falls by about a quarter over 500
+iterations).  The two error records agree, and so do the plans.  (On the
+Erdos-Renyi n=32768 workload the FP64 restatement caps on the same first three
+solves as this path: tests/test_gpu_accuracy.py.)"""
 
 import numpy as np
 import pytest
@@ -20,11 +20,11 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def test_capped_fp32_solve_is_the_fp32_error_floor():
+def test_capped_solves_cap_in_fp64_too():
     from cugal_b200.adjacency import Adjacency
     from cugal_b200.feature_extraction import Features
     from cugal_b200.pred import FrankWolfeEngine
-    from cugal_b200.synthetic import WORKLOADS, config_for, make_pair
+    from cugal_b200.synthetic import config_for, make_pair
     from oracle import fugal_torch64 as T
     src, tgt, _, w = make_pair("ba8192")
     n = src.number_of_nodes()
@@ -47,13 +47,12 @@ def test_capped_fp32_solve_is_the_fp32_error_floor():
     rec = T.sinkhorn_log_solve_(K, u, v, 500, 1e-4, 10, block=1024)
     P64 = torch.exp(K + u[:, None] + v[None, :])
     floor = n * 2.0 ** -24
-    err_exact = T.marginal_error(K, u32.clone(), v32.clone(), 1024)  # the FP32 duals' error evaluated in FP64
     diff = float((P32 - P64).abs().max().item())
-    print(f"\n[ba8192 step 6] FP32 stream: {prof.iteration_count} iterations, recorded errors min "
-          f"{min(prof.errors):.2e} last {prof.errors[-1]:.2e}; its duals' error in FP64 {err_exact:.2e}; "
-          f"FP64 solve: {rec.iterations} iterations, last error {rec.errors[-1]:.2e}; n 2^-24 = {floor:.2e}; "
-          f"max|P32 - P64| {diff:.2e}")
-    assert rec.iterations < 500 and rec.errors[-1] < 1e-4       # FP64 reaches the tolerance
-    assert prof.iteration_count == 500                          # FP32 runs to the cap ...
-    assert min(prof.errors) > 1e-4 and min(prof.errors) < 50 * floor  # ... stuck at the FP32 floor
-    assert diff < 1e-3
+    m = min(len(prof.errors), len(rec.errors))
+    print(f"\n[ba8192 step 6] this path: {prof.iteration_count} iterations, error {prof.errors[0]:.3e} -> "
+          f"{prof.errors[-1]:.3e}; FP64: {rec.iterations} iterations, error {rec.errors[0]:.3e} -> "
+          f"{rec.errors[-1]:.3e}; FP32 floor n 2^-24 = {floor:.1e}; max|P32 - P64| {diff:.2e}")
+    assert rec.iterations == 500 and prof.iteration_count == 500   # both run to the cap
+    assert rec.errors[-1] > 1e3 * floor                             # far above the FP32 floor
+    np.testing.assert_allclose(prof.errors[:m], rec.errors[:m], rtol=1e-2)
+    assert diff < 5e-3
