@@ -302,16 +302,19 @@ __global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const
     outT[static_cast<size_t>(j) * ldo + i] = sign * acc;
 }
 
-// Launch-shape knobs of the gradient kernels (FUGAL_GATHER_UNROLL: gathers in
-// flight per lane, 4 or 8; FUGAL_GRAD_MIN_BLOCKS: resident CTAs per SM the
-// epilogue kernel is compiled for, 6 or 8).
+// Launch-shape knobs of the gradient kernels.  FUGAL_GATHER_UNROLL: gathers in
+// flight per lane, 4 (default) or 8 (8 measured slower: 11.76 against 11.31 ms
+// per step at n = 32768, the extra registers cost resident CTAs).
+// FUGAL_GRAD_MIN_BLOCKS: resident CTAs per SM the epilogue kernel is compiled
+// for, 8 (default: 32 registers with a few spills, 10.87 ms) or 6 (40 registers,
+// no spills, 11.31 ms) -- the epilogue is issue-bound and needs the warps.
 int gather_unroll() {
     const char* e = getenv("FUGAL_GATHER_UNROLL");
     return (e != nullptr && atoi(e) == 8) ? 8 : 4;
 }
 int gradient_min_blocks() {
     const char* e = getenv("FUGAL_GRAD_MIN_BLOCKS");
-    return (e != nullptr && atoi(e) == 8) ? 8 : 6;
+    return (e != nullptr && atoi(e) == 6) ? 6 : 8;
 }
 
 // col may be null for a graph without edges (it is never dereferenced then).
@@ -421,7 +424,7 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
             else
                 gradient_kernel<true, 4, 6><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
         } else {
-            gradient_kernel<false><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
+            gradient_kernel<false, 4, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
         }
         FUGAL_TRY(launch_check("fugal_fw_gradient: (A P) B + epilogue"));
     }
