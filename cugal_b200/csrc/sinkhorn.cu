@@ -718,10 +718,7 @@ __device__ __forceinline__ float sum16(const float* r) {
 // after it has received the next exchange, which this CTA sends after a barrier
 // that follows every read of the slot.  A timed-out exchange is carried to the
 // next barrier vote.
-// WIDE (bit 0): a segment's 32 column duals come from TMEM in one 32-column load
-// (one wait) instead of two 16-column loads; (bit 1): the column sums are
-// updated 32 columns per load instead of 16.
-template <typename T, int EPT, int THREADS, bool BT, int POLY, int CL, int WIDE = 0>
+template <typename T, int EPT, int THREADS, bool BT, int POLY, int CL>
 __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) {
     constexpr int kRowThreads = THREADS;
     constexpr int kRowWarps = THREADS / 32;
@@ -736,8 +733,6 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     static_assert(kRowWarps == 16, "sum16 reduces 16 warp partials");
     static_assert(SEG <= kRowSeg, "segment larger than a stage");
     static_assert(CL == 1 || (CL == 2 && BT), "two-CTA rows keep the column duals in TMEM");
-    constexpr bool B32 = BT && (WIDE & 1) && EPS == 32;
-    constexpr bool A32 = (WIDE & 2) && EPT % 32 == 0;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t full[kMaxStages];
     __shared__ uint64_t xbar[2];
@@ -918,17 +913,10 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             okk = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
                             p.suspend_ns, p.wait_limit_ns) && okk;
             const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
-            float bseg[B32 ? 32 : 1];
-            if constexpr (B32) tmem_ld32(tb + sg * EPS, bseg);
 #pragma unroll
             for (int g0 = 0; g0 < G; g0 += 2) {
                 float2 b2[8];
-                if constexpr (B32) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) b2[q] = make_float2(bseg[8 * g0 + 2 * q], bseg[8 * g0 + 2 * q + 1]);
-                } else {
-                    b_pair(sg, g0, b2);
-                }
+                b_pair(sg, g0, b2);
 #pragma unroll
                 for (int gg = 0; gg < 2; ++gg) {
                     const int g = g0 + gg;
@@ -1125,32 +1113,17 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         // column sums of the row-normalised plan, accumulated in TMEM (one 16-column
         // chunk per load; batching two chunks per wait measured slower)
         const float2 w2 = make_float2(wr, wr);
-        if constexpr (A32) {
 #pragma unroll
-            for (int k = 0; k < EPT / 32; ++k) {
-                float acc[32];
-                tmem_ld32(tcol + 32 * k, acc);
+        for (int k = 0; k < EPT / 16; ++k) {
+            float acc[16];
+            tmem_ld16(tcol + 16 * k, acc);
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const float2 a2 = __ffma2_rn(y[16 * k + q], w2, make_float2(acc[2 * q], acc[2 * q + 1]));
-                    acc[2 * q] = a2.x;
-                    acc[2 * q + 1] = a2.y;
-                }
-                tmem_st32(tcol + 32 * k, acc);
+            for (int q = 0; q < 8; ++q) {
+                const float2 a2 = __ffma2_rn(y[8 * k + q], w2, make_float2(acc[2 * q], acc[2 * q + 1]));
+                acc[2 * q] = a2.x;
+                acc[2 * q + 1] = a2.y;
             }
-        } else {
-#pragma unroll
-            for (int k = 0; k < EPT / 16; ++k) {
-                float acc[16];
-                tmem_ld16(tcol + 16 * k, acc);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const float2 a2 = __ffma2_rn(y[8 * k + q], w2, make_float2(acc[2 * q], acc[2 * q + 1]));
-                    acc[2 * q] = a2.x;
-                    acc[2 * q + 1] = a2.y;
-                }
-                tmem_st16(tcol + 16 * k, acc);
-            }
+            tmem_st16(tcol + 16 * k, acc);
         }
     }
 
@@ -1629,7 +1602,6 @@ struct RowPlan {
     bool bt = true;
     int poly = 0;
     int cl = 1;      // CTAs per row block (a cluster when 2)
-    int wide = 0;    // 32-column TMEM accesses (row_wide)
     int groups = 0;  // row blocks (rows of column partials)
     int threads = 512;
     int ept = 0;
@@ -1642,42 +1614,27 @@ struct RowPlan {
 
 using RowKernelFn = void (*)(const RowArgs);
 
-template <typename T, bool BT, int POLY, int WIDE = 0>
+template <typename T, bool BT, int POLY>
 RowKernelFn row_kernel_typed(int ept, int cl) {
-    if (cl == 2) return row_sweep_kernel<T, 64, 512, BT, POLY, (BT ? 2 : 1), WIDE>;
-    return ept == 16 ? row_sweep_kernel<T, 16, 512, BT, POLY, 1, WIDE>
-                     : (ept == 32 ? row_sweep_kernel<T, 32, 512, BT, POLY, 1, WIDE>
-                                  : row_sweep_kernel<T, 64, 512, BT, POLY, 1, WIDE>);
+    if (cl == 2) return row_sweep_kernel<T, 64, 512, BT, POLY, (BT ? 2 : 1)>;
+    return ept == 16 ? row_sweep_kernel<T, 16, 512, BT, POLY, 1>
+                     : (ept == 32 ? row_sweep_kernel<T, 32, 512, BT, POLY, 1> : row_sweep_kernel<T, 64, 512, BT, POLY, 1>);
 }
 
 template <typename T>
-RowKernelFn row_kernel_dt(int ept, bool bt, int poly, int cl, int wide) {
+RowKernelFn row_kernel_dt(int ept, bool bt, int poly, int cl) {
     if (!bt) return row_kernel_typed<T, false, 0>(ept, 1);
     switch (poly) {
         case 4: return row_kernel_typed<T, true, 4>(ept, cl);
-        case 8:
-            switch (wide) {
-                case 1: return row_kernel_typed<T, true, 8, 1>(ept, cl);
-                case 2: return row_kernel_typed<T, true, 8, 2>(ept, cl);
-                case 3: return row_kernel_typed<T, true, 8, 3>(ept, cl);
-                default: return row_kernel_typed<T, true, 8, 0>(ept, cl);
-            }
+        case 8: return row_kernel_typed<T, true, 8>(ept, cl);
         default: return row_kernel_typed<T, true, 0>(ept, cl);
     }
 }
 
-RowKernelFn row_kernel_for(int dt, int ept, int threads, bool bt, int poly, int cl, int wide) {
+RowKernelFn row_kernel_for(int dt, int ept, int threads, bool bt, int poly, int cl) {
     (void)threads;
-    return dt == FUGAL_BF16 ? row_kernel_dt<__nv_bfloat16>(ept, bt, poly, cl, wide)
-                            : row_kernel_dt<__half>(ept, bt, poly, cl, wide);
-}
-
-// 32-column TMEM accesses in the row sweep (FUGAL_ROW_WIDE: bit 0 the column
-// duals, bit 1 the column sums; with one exponential pair in 8 on the FMA pipe).
-int row_wide() {
-    const char* e = getenv("FUGAL_ROW_WIDE");
-    const int v = e != nullptr ? atoi(e) : 0;
-    return (v >= 0 && v <= 3) ? v : 0;
+    return dt == FUGAL_BF16 ? row_kernel_dt<__nv_bfloat16>(ept, bt, poly, cl)
+                            : row_kernel_dt<__half>(ept, bt, poly, cl);
 }
 
 // Share of the row sweep's fast-path exponentials evaluated on the FMA pipe:
@@ -1729,7 +1686,6 @@ fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool s
     if (rp.ept == 48) rp.ept = 64;
     const size_t stage_bytes = static_cast<size_t>(rp.threads) * std::min(rp.ept, kRowSeg / rp.threads) * 2;
     rp.poly = rp.bt ? row_poly() : 0;
-    rp.wide = rp.poly == 8 ? row_wide() : 0;
     // column duals of every covered column, unless they live in TMEM
     const size_t fixed = rp.bt ? 0 : static_cast<size_t>(rp.threads) * rp.ept * 4;
     const int64_t room = static_cast<int64_t>(max_smem_optin()) - 1024 - static_cast<int64_t>(fixed);
@@ -1737,7 +1693,7 @@ fugal_status make_row_plan(int64_t n, int dt, int64_t n_pad, RowPlan& rp, bool s
     if (rp.stages < 2) return FUGAL_OK;
     rp.smem = fixed + rp.stages * stage_bytes;
     int groups = static_cast<int>(std::min<int64_t>(sm_count() / rp.cl, n));
-    RowKernelFn fn = row_kernel_for(dt, rp.ept, rp.threads, rp.bt, rp.poly, rp.cl, rp.wide);
+    RowKernelFn fn = row_kernel_for(dt, rp.ept, rp.threads, rp.bt, rp.poly, rp.cl);
     if (set_attributes) {
         FUGAL_TRY(cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp.smem),
                              "sinkhorn: row sweep shared memory"));
@@ -2059,7 +2015,7 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
             {
                 LaunchScope scope(FUGAL_KERNEL_SWEEP, stream);
                 RowKernelFn fn = row_kernel_for(p.stream_dtype, rowplan.ept, rowplan.threads, rowplan.bt,
-                                                rowplan.poly, rowplan.cl, rowplan.wide);
+                                                rowplan.poly, rowplan.cl);
                 if (rowplan.cl == 1) {
                     fn<<<rowplan.ctas, rowplan.threads, rowplan.smem, stream>>>(ra);
                     status = launch_check("sinkhorn: row sweep");

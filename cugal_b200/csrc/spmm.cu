@@ -188,10 +188,7 @@ struct EpilogueArgs {
 // rows i0 .. i0+127 to a base-2 (max, sum) pair, x = out log2 e: M = max x,
 // S = sum 2^(x - M), stored at colpart[blockIdx.y][j] (the first column update
 // of the Sinkhorn solve merges them instead of reading the cost again).
-// SQ: the distance's square root as sqrt.approx (the reference's distance kernel
-// is compiled with --use_fast_math, cuda_kernels/setup.py:19) instead of the
-// IEEE-rounded one.
-template <bool COLSTATS, int U = 4, int MINB = 6, bool SQ = false>
+template <bool COLSTATS, int U = 4, int MINB = 6>
 __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int* __restrict__ rp,
                                                                 const int* __restrict__ col,
                                                                 const float* __restrict__ Tt, long long ldt, int n,
@@ -243,13 +240,7 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
                 const float4 f1 = fi[ii];
                 const float d0 = __fsub_rn(f1.x, f2.x), d1 = __fsub_rn(f1.y, f2.y);
                 const float d2 = __fsub_rn(f1.z, f2.z), d3 = __fsub_rn(f1.w, f2.w);
-                const float ss = __fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))));
-                float dist;
-                if constexpr (SQ)
-                    asm("sqrt.approx.f32 %0, %1;" : "=f"(dist) : "f"(ss));
-                else
-                    dist = __fsqrt_rn(ss);
-                g = __fadd_rn(g, dist);
+                g = __fadd_rn(g, __fsqrt_rn(__fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))))));
             } else if (ep.D != nullptr) {
                 g = __fadd_rn(g, ep.D[static_cast<size_t>(i) * ep.ldd + j]);
             }
@@ -320,10 +311,6 @@ __global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const
 int gather_unroll() {
     const char* e = getenv("FUGAL_GATHER_UNROLL");
     return (e != nullptr && atoi(e) == 8) ? 8 : 4;
-}
-bool gradient_sqrt_approx() {
-    const char* e = getenv("FUGAL_GRAD_SQRT_APPROX");
-    return e != nullptr && atoi(e) != 0;
 }
 int gradient_min_blocks() {
     const char* e = getenv("FUGAL_GRAD_MIN_BLOCKS");
@@ -432,8 +419,6 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
                 gradient_kernel<true, 8, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else if (unroll == 8)
                 gradient_kernel<true, 8, 6><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
-            else if (minb == 8 && gradient_sqrt_approx())
-                gradient_kernel<true, 4, 8, true><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else if (minb == 8)
                 gradient_kernel<true, 4, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else
