@@ -180,3 +180,42 @@ def test_er32768_full_schedule_node_accuracy_against_fp64():
               f"{np.mean(trace.sinkhorn_iterations):.2f}, capped solves "
               f"{int(np.sum(np.array(trace.sinkhorn_iterations) >= 500))}")
         assert abs(acc - acc64) <= 0.005
+
+
+def test_ba8192_full_schedule_against_fp64():
+    """Barabasi-Albert n=8192 (m 5, seed 1, 5% noise), the plain FP32 drop-in
+    path with SCIPY rounding, against the FP64 restatement over the full
+    15 x 10 schedule (its plan rounded by scipy): node accuracy and objective."""
+    import scipy.optimize
+    from oracle import fugal_torch64 as T
+    from cugal_b200.adjacency import Adjacency
+    from cugal_b200.pred import align
+    from cugal_b200.synthetic import config_for, make_pair
+    src, tgt, perm, w = make_pair("ba8192")
+    A_csr, B_csr = O.csr_from_graph(src), O.csr_from_graph(tgt)
+    F1 = O.features_cuda_semantics(*A_csr).astype(np.float64)
+    F2 = O.features_cuda_semantics(*B_csr).astype(np.float64)
+    trace = T.Trace()
+    P64 = T.find_quasi_permutation_matrix(A_csr, B_csr, F1, F2, reg=1e-3, iter_count=15, fw_iter_count=10,
+                                          sinkhorn_iterations=500, threshold=1e-4, eval_freq=10, mu=1.0,
+                                          device="cuda", block=1024, trace=trace)
+    n = P64.shape[0]
+    A = T.csr_tensor(*A_csr, n, "cuda")
+    B = T.csr_tensor(*B_csr, n, "cuda")
+    f1, f2 = torch.as_tensor(F1, device="cuda"), torch.as_tensor(F2, device="cuda")
+    obj64 = T.objective(A, B, P64, f1, f2, 14.0, 1024)["objective"]
+    cols64 = scipy.optimize.linear_sum_assignment(P64.cpu().numpy(), maximize=True)[1]
+    acc64 = float(np.mean(cols64 == perm))
+    del P64
+    torch.cuda.empty_cache()
+    config = config_for(w, device="cuda")
+    P, cols, _ = align(Adjacency.from_graph(src, "cuda"), Adjacency.from_graph(tgt, "cuda"), config)
+    cols = cols.cpu().numpy() if isinstance(cols, torch.Tensor) else np.asarray(cols)
+    acc = float(np.mean(cols == perm))
+    obj = T.objective(A, B, P.double(), f1, f2, 14.0, 1024)["objective"]
+    rel = abs(obj - obj64) / abs(obj64)
+    print(f"\n[ba8192 full schedule fp32, SCIPY] node accuracy {acc:.4f} vs FP64 {acc64:.4f}; objective {obj:.4f} vs "
+          f"{obj64:.4f} (rel {rel:.2e}); same column {float(np.mean(cols == cols64)):.4f}; FP64 mean iterations "
+          f"{np.mean(trace.sinkhorn_iterations):.1f}, capped {int(np.sum(np.array(trace.sinkhorn_iterations) >= 500))}")
+    assert abs(acc - acc64) <= 0.005
+    assert rel <= 1e-2
