@@ -17,10 +17,14 @@ the alignment path has no exchange step), timing is the max over ranks and
 
 The JSON line also carries the roofline of the dominant kernel (the BF16 sweep:
 algorithmic bytes = one read of the n x ld 16-bit cost per sweep that ran, over
-the CUDA-event time of all its launches in the timed region), the
-host CPU baseline (the reference's FP64 CPU Sinkhorn iteration timed on a block
-of rows, extrapolated), SM clocks sampled during the timed region, and the
-number of this library's kernel launches in the timed region.
+the CUDA-event time of all its launches in the timed region), the same
+alignment with the FP32 stream (``fp32_path``: seconds, e2e, node accuracy and
+the BF16 speed-up over it), the reference's own FP32 GPU path timed as whole
+Frank-Wolfe steps on its compiled kernels and extrapolated
+(``reference_gpu_fp32``), the host CPU baseline (the reference's FP64 CPU
+Sinkhorn iteration timed on a block of rows, scaled by the FP64 restatement's
+iteration counts on the workload), SM clocks sampled during the timed region,
+and the number of this library's kernel launches in the timed region.
 """
 
 from __future__ import annotations
