@@ -188,7 +188,11 @@ struct EpilogueArgs {
 // rows i0 .. i0+127 to a base-2 (max, sum) pair, x = out log2 e: M = max x,
 // S = sum 2^(x - M), stored at colpart[blockIdx.y][j] (the first column update
 // of the Sinkhorn solve merges them instead of reading the cost again).
-template <bool COLSTATS, int U = 4, int MINB = 6>
+// PK: chunks of four in-range columns with features take a packed path -- the
+// FP32 arithmetic of two columns per FP32x2 instruction (the same IEEE operations
+// in the same order, so the same results) and the row duals read from shared
+// memory; other chunks take the scalar path.
+template <bool COLSTATS, int U = 4, int MINB = 6, bool PK = true>
 __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int* __restrict__ rp,
                                                                 const int* __restrict__ col,
                                                                 const float* __restrict__ Tt, long long ldt, int n,
@@ -198,9 +202,14 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
     __shared__ float4 fi[kTileCols];
     __shared__ float4 fj[kTileRows];
     __shared__ float2 cst[COLSTATS ? kWarps : 1][kTileRows];
+    __shared__ double us[kTileCols];
     const int j0 = blockIdx.x * kTileRows;   // gathered rows: target nodes j
     const int i0 = blockIdx.y * kTileCols;   // lanes: source nodes i
     const bool has_f = ep.fs != nullptr;
+    if constexpr (PK) {
+        for (int q = threadIdx.x; q < kTileCols; q += kSpmmThreads)
+            us[q] = (ep.U != nullptr && i0 + q < n) ? ep.U[i0 + q] : 0.0;
+    }
     if (has_f) {
         for (int q = threadIdx.x; q < kTileCols; q += kSpmmThreads)
             fi[q] = (i0 + q < n) ? reinterpret_cast<const float4*>(ep.fs)[i0 + q] : make_float4(0, 0, 0, 0);
@@ -219,6 +228,51 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
     float xmax = -INFINITY;
     for (int q = warp; q < kChunks; q += kWarps) {
         if (i0 + 4 * q >= n || j >= n) break;
+        if (PK && has_f && i0 + 4 * q + 3 < n) {
+            const float4 apb4 = tile.at(lane, q);
+            const float2 m2 = make_float2(-2.0f, -2.0f);
+            float2 g2[2] = {__fmul2_rn(m2, make_float2(apb4.x, apb4.y)), __fmul2_rn(m2, make_float2(apb4.z, apb4.w))};
+            const int ib = i0 + 4 * q;
+            if (use_p) {
+                const float* pc = ep.P + static_cast<size_t>(ib) * ep.ldp + j;
+                const float2 lam2 = make_float2(lam, lam), one2 = make_float2(1.0f, 1.0f);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float2 p2 = make_float2(pc[(2 * h) * ep.ldp], pc[(2 * h + 1) * ep.ldp]);
+                    // lam (1 - 2p): 1 + (-2p) is 1 - 2p exactly
+                    g2[h] = __fadd2_rn(g2[h], __fmul2_rn(lam2, __fadd2_rn(one2, __fmul2_rn(m2, p2))));
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) g2[h] = __fadd2_rn(g2[h], make_float2(0.f, 0.f));
+            }
+            float o[4];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const float4 fa = fi[4 * q + 2 * h], fb = fi[4 * q + 2 * h + 1];
+                const float2 d0 = __fadd2_rn(make_float2(fa.x, fb.x), make_float2(-f2.x, -f2.x));
+                const float2 d1 = __fadd2_rn(make_float2(fa.y, fb.y), make_float2(-f2.y, -f2.y));
+                const float2 d2 = __fadd2_rn(make_float2(fa.z, fb.z), make_float2(-f2.z, -f2.z));
+                const float2 d3 = __fadd2_rn(make_float2(fa.w, fb.w), make_float2(-f2.w, -f2.w));
+                float2 ss = __fmul2_rn(d0, d0);
+                ss = __ffma2_rn(d1, d1, ss);
+                ss = __ffma2_rn(d2, d2, ss);
+                ss = __ffma2_rn(d3, d3, ss);
+                const float2 g = __fadd2_rn(g2[h], make_float2(__fsqrt_rn(ss.x), __fsqrt_rn(ss.y)));
+                o[2 * h] = static_cast<float>(ep.out_scale * static_cast<double>(g.x) + (us[4 * q + 2 * h] + vj));
+                o[2 * h + 1] =
+                    static_cast<float>(ep.out_scale * static_cast<double>(g.y) + (us[4 * q + 2 * h + 1] + vj));
+            }
+            float* oc = ep.out + static_cast<size_t>(ib) * ep.ldo + j;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) oc[t * ep.ldo] = o[t];
+            if constexpr (COLSTATS) {
+                const float4 x = make_float4(o[0] * kLog2e, o[1] * kLog2e, o[2] * kLog2e, o[3] * kLog2e);
+                xmax = fmaxf(xmax, fmaxf(fmaxf(x.x, x.y), fmaxf(x.z, x.w)));
+                tile.at(lane, q) = x;
+            }
+            continue;
+        }
         const float4 apb4 = tile.at(lane, q);
         const float apbs[4] = {apb4.x, apb4.y, apb4.z, apb4.w};
         float xs[4];
@@ -311,6 +365,10 @@ __global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const
 int gather_unroll() {
     const char* e = getenv("FUGAL_GATHER_UNROLL");
     return (e != nullptr && atoi(e) == 8) ? 8 : 4;
+}
+bool gradient_packed() {
+    const char* e = getenv("FUGAL_GRAD_PACKED");
+    return !(e != nullptr && atoi(e) == 0);
 }
 int gradient_min_blocks() {
     const char* e = getenv("FUGAL_GRAD_MIN_BLOCKS");
@@ -419,6 +477,8 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
                 gradient_kernel<true, 8, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else if (unroll == 8)
                 gradient_kernel<true, 8, 6><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
+            else if (minb == 8 && !gradient_packed())
+                gradient_kernel<true, 4, 8, false><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else if (minb == 8)
                 gradient_kernel<true, 4, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else
