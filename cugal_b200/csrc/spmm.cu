@@ -49,9 +49,14 @@ struct Tile {
 // rows are 16-byte aligned (VEC), else scalar loads guarded by n.  (Loads that
 // skip L1 allocation, ld.global.nc.L1::no_allocate, made the pair of gradient
 // kernels 50% slower at n = 32768.)
+// Row offset k * ldx as one 32 x 32 -> 64-bit multiply (k >= 0 and ldx < 2^32).
+__device__ __forceinline__ unsigned long long row_offset(int k, long long ldx) {
+    return static_cast<unsigned long long>(static_cast<unsigned>(k)) * static_cast<unsigned>(ldx);
+}
+
 template <bool VEC>
 __device__ __forceinline__ float4 load4(const float* __restrict__ X, long long ldx, int k, int c, int n) {
-    const float* p = X + static_cast<size_t>(k) * ldx + c;
+    const float* p = X + row_offset(k, ldx) + c;
     if (VEC) return __ldg(reinterpret_cast<const float4*>(p));
     float4 v;
     v.x = __ldg(p);
@@ -75,6 +80,7 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
         hi = __fadd2_rn(hi, make_float2(v.z, v.w));
     };
     const int lane = threadIdx.x & 31;
+    const float* Xc = X + c;  // this lane's columns; rows are offset from here
     const int rs = rp[row], re = rp[row + 1];
     for (int e = rs; e < re; e += 32) {
         const int cnt = min(32, re - e);
@@ -87,14 +93,14 @@ __device__ __forceinline__ float4 gather_row(const int* __restrict__ rp, const i
             if (c_ok) {
                 float4 v[U];
 #pragma unroll
-                for (int t = 0; t < U; ++t) v[t] = load4<VEC>(X, ldx, k[t], c, n);
+                for (int t = 0; t < U; ++t) v[t] = load4<VEC>(Xc, ldx, k[t], 0, n - c);
 #pragma unroll
                 for (int t = 0; t < U; ++t) add(v[t]);
             }
         }
         for (; q < cnt; ++q) {
             const int k = __shfl_sync(0xffffffffu, idx, q);
-            if (c_ok) add(load4<VEC>(X, ldx, k, c, n));
+            if (c_ok) add(load4<VEC>(Xc, ldx, k, 0, n - c));
         }
     }
     return make_float4(lo.x, lo.y, hi.x, hi.y);
@@ -137,10 +143,11 @@ __global__ void __launch_bounds__(kSpmmThreads) spmm_kernel(const int* __restric
             const float4 v = tile.at(lane, q);
             const int cg = c0 + 4 * q;
             if (rg < n) {
-                if (cg + 0 < n) out[static_cast<size_t>(cg + 0) * ldo + rg] = v.x;
-                if (cg + 1 < n) out[static_cast<size_t>(cg + 1) * ldo + rg] = v.y;
-                if (cg + 2 < n) out[static_cast<size_t>(cg + 2) * ldo + rg] = v.z;
-                if (cg + 3 < n) out[static_cast<size_t>(cg + 3) * ldo + rg] = v.w;
+                float* o = out + row_offset(cg, ldo) + rg;
+                if (cg + 0 < n) o[0] = v.x;
+                if (cg + 1 < n) o[ldo] = v.y;
+                if (cg + 2 < n) o[2 * ldo] = v.z;
+                if (cg + 3 < n) o[3 * ldo] = v.w;
             }
         }
     } else {
@@ -234,7 +241,7 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
             float2 g2[2] = {__fmul2_rn(m2, make_float2(apb4.x, apb4.y)), __fmul2_rn(m2, make_float2(apb4.z, apb4.w))};
             const int ib = i0 + 4 * q;
             if (use_p) {
-                const float* pc = ep.P + static_cast<size_t>(ib) * ep.ldp + j;
+                const float* pc = ep.P + row_offset(ib, ep.ldp) + j;
                 const float2 lam2 = make_float2(lam, lam), one2 = make_float2(1.0f, 1.0f);
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
@@ -263,7 +270,7 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
                 o[2 * h + 1] =
                     static_cast<float>(ep.out_scale * static_cast<double>(g.y) + (us[4 * q + 2 * h + 1] + vj));
             }
-            float* oc = ep.out + static_cast<size_t>(ib) * ep.ldo + j;
+            float* oc = ep.out + row_offset(ib, ep.ldo) + j;
 #pragma unroll
             for (int t = 0; t < 4; ++t) oc[t * ep.ldo] = o[t];
             if constexpr (COLSTATS) {
@@ -394,6 +401,8 @@ extern "C" fugal_status fugal_adjacency_matmul(const int32_t* col_indices, const
     FUGAL_TRY(check_csr(row_pointers, col_indices, n, "fugal_adjacency_matmul"));
     if (M == nullptr || out == nullptr) return fail(FUGAL_BAD_ARGUMENT, "fugal_adjacency_matmul: null matrix");
     if (ldm < n || ldo < n) return fail(FUGAL_BAD_SHAPE, "fugal_adjacency_matmul: leading dimension < n");
+    if (ldm >= (1ll << 32) || ldo >= (1ll << 32))
+        return fail(FUGAL_BAD_SHAPE, "fugal_adjacency_matmul: leading dimension >= 2^32");
     const float sign = negate ? -1.f : 1.f;
     LaunchScope scope(FUGAL_KERNEL_OTHER, stream);
     if (!m_transposed) {
@@ -441,6 +450,7 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
     if (D != nullptr && ldd < n) return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: ldd < n");
     if (ldp < n || ldo < n || (ldp % 4) != 0 || !aligned16(P))
         return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: P needs ld >= n, ld %% 4 == 0, 16-byte base");
+    if (ldp >= (1ll << 32) || ldo >= (1ll << 32)) return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: ld >= 2^32");
     if (source_features && (!aligned16(source_features) || !aligned16(target_features)))
         return fail(FUGAL_BAD_SHAPE, "fugal_fw_gradient: feature rows must be 16-byte aligned");
     if (column_partials != nullptr && (ldc < n || (reinterpret_cast<uintptr_t>(column_partials) & 7u) != 0))
