@@ -377,8 +377,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     __syncthreads();
     cluster_sync();  // every peer's barriers exist before the first remote transaction
 
-    auto issue = [&](int bt) {
-        const int s = bt % p.stages;
+    auto issue = [&](int bt, int s) {  // batch bt into stage s (bt % stages == s)
         const int r0 = row_begin + bt * R;
         const int rows = min(R, row_end - r0);
         unsigned char* dst = stage_base + s * stage_bytes;
@@ -393,13 +392,13 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     int issued = 0;
     if (tid == 0) {
         issued = min(p.stages, nbatch);
-        for (int bt = 0; bt < issued; ++bt) issue(bt);
+        for (int bt = 0; bt < issued; ++bt) issue(bt, bt);
     }
-    // Stage of batch bt is no longer read: refill it with batch bt + stages (thread 0).
-    auto release = [&](int bt) {
+    // Stage s of batch bt is no longer read: refill it with batch bt + stages (thread 0).
+    auto release = [&](int bt, int s) {
         if (tid == 0 && bt + p.stages < nbatch) {
             fence_proxy_async_smem();
-            issue(bt + p.stages);
+            issue(bt + p.stages, s);
             ++issued;
         }
     };
@@ -429,9 +428,17 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
     int xuse = 0;
     bool alive = true;
     int bt = 0;
+    // stage and barrier parity of batch bt, advanced per batch (no division in the loop)
+    int s_next = 0;
+    uint32_t ph_next = 0u;
     for (; bt < nbatch; ++bt) {
-        const int s = bt % p.stages;
-        if (!agree(mbar_wait(&full[s], static_cast<uint32_t>((bt / p.stages) & 1), &st->status, p.suspend_ns))) {
+        const int s = s_next;
+        const uint32_t ph = ph_next;
+        if (++s_next == p.stages) {
+            s_next = 0;
+            ph_next ^= 1u;
+        }
+        if (!agree(mbar_wait(&full[s], ph, &st->status, p.suspend_ns))) {
             alive = false;
             break;
         }
@@ -505,7 +512,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                     anew[r] = a_old[r] - __log2f(S[r]) * kLn2;  // -(M_ref + ln S)
                     wr[r] = __frcp_rn(S[r]);
                 }
-                if (!ABSORB) release(bt);
+                if (!ABSORB) release(bt, s);
             }
         }
         if (!fast_ok) {
@@ -546,7 +553,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 512 / THREADS))
                 alive = false;
                 break;
             }
-            release(bt);  // the stage is not read again: x stays in registers
+            release(bt, s);  // the stage is not read again: x stays in registers
             float M2[R], sm[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -835,8 +842,32 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     }
     tmem_wait_st();
 
-    auto issue = [&](int u) {
-        const int s = u % p.stages;
+    // Stage ring cursor: the stage and barrier parity of the first unit of a row,
+    // advanced row by row (no division by the runtime stage count in the loop).
+    struct Cursor {
+        int s;
+        uint32_t ph;
+    };
+    const int NST = p.stages;
+    auto unit_at = [&](Cursor c, int sg, int& st_idx, uint32_t& par_bit) {
+        st_idx = c.s + sg;
+        par_bit = c.ph;
+        if (st_idx >= NST) {
+            st_idx -= NST;
+            par_bit ^= 1u;
+        }
+    };
+    auto next_rows = [&](Cursor c, int k) {
+        c.s += k * NSEG;
+        while (c.s >= NST) {
+            c.s -= NST;
+            c.ph ^= 1u;
+        }
+        return c;
+    };
+    Cursor cur{0, 0u};
+
+    auto issue = [&](int u, int s) {  // unit u into stage s (u % S == s)
         const int row = row_begin + u / NSEG;
         const int seg = u % NSEG;
         const int cols = min(SEG, p.n_copy - col0 - seg * SEG);
@@ -853,15 +884,18 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     if (tid == 0) {
         fence_proxy_async_smem();  // the zero fill above precedes the copies
         issued = min(p.stages, units);
-        for (int u = 0; u < issued; ++u) issue(u);
+        for (int u = 0; u < issued; ++u) issue(u, u);
     }
-    auto release = [&](int r) {
+    auto release = [&](int r, Cursor c) {  // c: the cursor of row r
         if (tid == 0) {
             fence_proxy_async_smem();
-            for (int s = 0; s < NSEG; ++s) {
-                const int u = r * NSEG + s + p.stages;
+            for (int sg = 0; sg < NSEG; ++sg) {
+                const int u = r * NSEG + sg + NST;
                 if (u < units) {
-                    issue(u);
+                    int si;
+                    uint32_t ph;
+                    unit_at(c, sg, si, ph);
+                    issue(u, si);
                     ++issued;
                 }
             }
@@ -906,13 +940,14 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
 
     // Fast-path exponentials of local row rr (its stages waited for here):
     // yy = 2^(L log2e + b) against the absorbed frame, s2 / t2 partial row sums.
-    auto row_fast = [&](int rr, float2(&yy)[H], float2& s2, float2& t2, bool& okk) {
+    auto row_fast = [&](Cursor c, float2(&yy)[H], float2& s2, float2& t2, bool& okk) {
 #pragma unroll
         for (int sg = 0; sg < NSEG; ++sg) {
-            const int u = rr * NSEG + sg;
-            okk = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
-                            p.suspend_ns, p.wait_limit_ns) && okk;
-            const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
+            int si;
+            uint32_t ph;
+            unit_at(c, sg, si, ph);
+            okk = mbar_wait(&full[si], ph, &st->status, p.suspend_ns, p.wait_limit_ns) && okk;
+            const T* stage = reinterpret_cast<const T*>(stage_base + si * stage_bytes);
 #pragma unroll
             for (int g0 = 0; g0 < G; g0 += 2) {
                 float2 b2[8];
@@ -960,7 +995,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                 for (int k = 0; k < RB; ++k) {
                     float2 sa = make_float2(0.f, 0.f), ta = sa;
                     if (k < nr) {
-                        row_fast(r + k, yg[k], sa, ta, ok);
+                        row_fast(next_rows(cur, k), yg[k], sa, ta, ok);
                     } else {
 #pragma unroll
                         for (int h = 0; h < H; ++h) yg[k][h] = make_float2(0.f, 0.f);
@@ -991,7 +1026,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                 if (!in_range) break;  // uniform
 #pragma unroll
                 for (int k = 0; k < RB; ++k) {
-                    if (k < nr) release(r + k);
+                    if (k < nr) release(r + k, next_rows(cur, k));
                     wk[k] = k < nr ? __frcp_rn(S[k]) : 0.f;
                     if (tid == 0 && k < nr) p.a[row_begin + r + k] = -__log2f(S[k]) * kLn2;
                 }
@@ -1009,6 +1044,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                     }
                     tmem_st16(tcol + 16 * c, acc);
                 }
+                cur = next_rows(cur, nr);
             }
         }
     }
@@ -1016,6 +1052,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
     for (; r < nrows; ++r) {
         const int row = row_begin + r;
         const int par = r & 1;
+        const Cursor rc = cur;
         bool ok = true;
         float2 y[H];
         float anew = 0.f, wr = 0.f;
@@ -1023,7 +1060,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         if (!exact_only) {
             // ---- fast path: 2^(L log2e + b) against the absorbed frame
             float2 s2 = make_float2(0.f, 0.f), t2 = make_float2(0.f, 0.f);
-            row_fast(r, y, s2, t2, ok);
+            row_fast(rc, y, s2, t2, ok);
             const float2 u2 = __fadd2_rn(s2, t2);
             const float part = warp_sum(u2.x + u2.y);
             if (lane == 0) red_s[par][warp] = part;
@@ -1038,7 +1075,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             }
             fast_ok = S > 1e-30f && S < 1e30f;  // uniform
             if (fast_ok) {
-                release(r);
+                release(r, rc);
                 anew = -__log2f(S) * kLn2;
                 wr = __frcp_rn(S);
             }
@@ -1051,11 +1088,11 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             float mx = -INFINITY;
 #pragma unroll
             for (int sg = 0; sg < NSEG; ++sg) {
-                const int u = r * NSEG + sg;
-                if (exact_only)
-                    ok = mbar_wait(&full[u % p.stages], static_cast<uint32_t>((u / p.stages) & 1), &st->status,
-                                   p.suspend_ns, p.wait_limit_ns) && ok;
-                const T* stage = reinterpret_cast<const T*>(stage_base + (u % p.stages) * stage_bytes);
+                int si;
+                uint32_t ph;
+                unit_at(rc, sg, si, ph);
+                if (exact_only) ok = mbar_wait(&full[si], ph, &st->status, p.suspend_ns, p.wait_limit_ns) && ok;
+                const T* stage = reinterpret_cast<const T*>(stage_base + si * stage_bytes);
 #pragma unroll
                 for (int g0 = 0; g0 < G; g0 += 2) {
                     float2 b2[8];
@@ -1099,7 +1136,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
                 alive = false;
                 break;
             }
-            release(r);
+            release(r, rc);
             float S = sum16(red_s[par]);
             if constexpr (CL > 1) {
                 const float Sp = swap_with_peer(S);
@@ -1125,6 +1162,7 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
             }
             tmem_st16(tcol + 16 * k, acc);
         }
+        cur = next_rows(cur, 1);
     }
 
     // per-CTA column sums -> partials[cta][col]
