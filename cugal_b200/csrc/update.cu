@@ -38,17 +38,14 @@ __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict
                                                                double reg, double* gap) {
     __shared__ double red[32];
     constexpr int kChunk = kEwThreads * 4;
-    const int chunks = (n + kChunk - 1) / kChunk;
-    const long long units = static_cast<long long>(n) * chunks;
     double g = 0.0;
-    for (long long w = blockIdx.x; w < units; w += gridDim.x) {
-        const int i = static_cast<int>(w / chunks);
-        const int j0 = static_cast<int>(w % chunks) * kChunk + threadIdx.x * 4;
-        if (j0 >= n) continue;
-        const float ui = u[i];
-        const double Ui = U ? U[i] : 0.0;
-        float* prow = P + static_cast<size_t>(i) * ldp;
-        const float* lrow = L + static_cast<size_t>(i) * ldl;
+    // rows grid-strided, each row's columns in chunks of kChunk (no division per chunk)
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+      const float ui = u[i];
+      const double Ui = U ? U[i] : 0.0;
+      float* prow = P + static_cast<size_t>(i) * ldp;
+      const float* lrow = L + static_cast<size_t>(i) * ldl;
+      for (int j0 = threadIdx.x * 4; j0 < n; j0 += kChunk) {
         if (j0 + 4 <= n) {
             const float4 l4 = *reinterpret_cast<const float4*>(lrow + j0);
             float4 p4 = *reinterpret_cast<float4*>(prow + j0);
@@ -73,6 +70,7 @@ __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict
                 prow[j] = fmaf(alpha, diff, prow[j]);
             }
         }
+      }
     }
     g = block_sum(g, red);
     if (threadIdx.x == 0) atomicAdd(gap, g);
@@ -224,8 +222,7 @@ extern "C" fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const 
     FUGAL_TRY(cuda_check(cudaMemsetAsync(gap, 0, sizeof(double), stream), "fugal_fw_update: clear gap"));
     {
         LaunchScope scope(FUGAL_KERNEL_UPDATE, stream);
-        const int64_t units = n * ((n + kEwThreads * 4 - 1) / (kEwThreads * 4));
-        const int blocks = static_cast<int>(std::min<int64_t>(units, static_cast<int64_t>(sm_count()) * 8));
+        const int blocks = static_cast<int>(std::min<int64_t>(n, static_cast<int64_t>(sm_count()) * 8));
         fw_update_kernel<<<blocks, kEwThreads, 0, stream>>>(P, ldp, cost32, ld32, u, v, U, V, static_cast<int>(n),
                                                             static_cast<float>(alpha), regularization, gap);
         FUGAL_TRY(launch_check(who));
