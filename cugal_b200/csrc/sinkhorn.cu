@@ -876,8 +876,9 @@ __global__ void __launch_bounds__(THREADS, 1) row_sweep_kernel(const RowArgs p) 
         mbar_arrive_expect_tx(&full[s], bytes + unmet);
         if (bytes > 0)
             bulk_load(stage_base + s * stage_bytes,
-                      static_cast<const T*>(p.L) + static_cast<size_t>(row) * p.ld + col0 +
-                          static_cast<size_t>(seg) * SEG,
+                      static_cast<const T*>(p.L) +
+                          static_cast<unsigned long long>(static_cast<unsigned>(row)) * static_cast<unsigned>(p.ld) +
+                          col0 + static_cast<size_t>(seg) * SEG,
                       bytes, &full[s]);
     };
     int issued = 0;
@@ -1896,6 +1897,8 @@ extern "C" fugal_status fugal_sinkhorn_solve(const fugal_solve_params* prm, void
         return fail(FUGAL_BAD_ARGUMENT, "fugal_sinkhorn_solve: max_iterations and eval_freq must be positive");
     if (p.ld32 < n || (p.ld32 % 4) != 0 || !aligned16(p.cost32))
         return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_solve: cost32 needs ld >= n, ld %% 4 == 0, 16-byte base");
+    if (p.ld32 >= (1ll << 32) || (use16 && p.ld16 >= (1ll << 32)))
+        return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_solve: leading dimensions must be below 2^32");
     if (use16 && (p.ld16 < n || (p.ld16 % 8) != 0 || !aligned16(p.cost16)))
         return fail(FUGAL_BAD_SHAPE, "fugal_sinkhorn_solve: cost16 needs ld >= n, ld %% 8 == 0, 16-byte base");
     if (use16 && (p.fp32_warmup_sweeps < 0 || p.reabsorb_every <= 0 || p.polish_sweeps < 0))

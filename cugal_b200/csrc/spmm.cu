@@ -199,7 +199,10 @@ struct EpilogueArgs {
 // FP32 arithmetic of two columns per FP32x2 instruction (the same IEEE operations
 // in the same order, so the same results) and the row duals read from shared
 // memory; other chunks take the scalar path.
-template <bool COLSTATS, int U = 4, int MINB = 6, bool PK = true>
+// SQ (packed path only): the distance's square root as sqrt.approx, the form the
+// reference's distance kernel is built with (--use_fast_math,
+// cuda_kernels/setup.py:19), instead of the IEEE-rounded one.
+template <bool COLSTATS, int U = 4, int MINB = 6, bool PK = true, bool SQ = false>
 __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int* __restrict__ rp,
                                                                 const int* __restrict__ col,
                                                                 const float* __restrict__ Tt, long long ldt, int n,
@@ -265,7 +268,14 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
                 ss = __ffma2_rn(d1, d1, ss);
                 ss = __ffma2_rn(d2, d2, ss);
                 ss = __ffma2_rn(d3, d3, ss);
-                const float2 g = __fadd2_rn(g2[h], make_float2(__fsqrt_rn(ss.x), __fsqrt_rn(ss.y)));
+                float2 dist;
+                if constexpr (SQ) {
+                    asm("sqrt.approx.f32 %0, %1;" : "=f"(dist.x) : "f"(ss.x));
+                    asm("sqrt.approx.f32 %0, %1;" : "=f"(dist.y) : "f"(ss.y));
+                } else {
+                    dist = make_float2(__fsqrt_rn(ss.x), __fsqrt_rn(ss.y));
+                }
+                const float2 g = __fadd2_rn(g2[h], dist);
                 o[2 * h] = static_cast<float>(ep.out_scale * static_cast<double>(g.x) + (us[4 * q + 2 * h] + vj));
                 o[2 * h + 1] =
                     static_cast<float>(ep.out_scale * static_cast<double>(g.y) + (us[4 * q + 2 * h + 1] + vj));
@@ -372,6 +382,10 @@ __global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const
 int gather_unroll() {
     const char* e = getenv("FUGAL_GATHER_UNROLL");
     return (e != nullptr && atoi(e) == 8) ? 8 : 4;
+}
+bool gradient_sqrt_approx() {
+    const char* e = getenv("FUGAL_GRAD_SQRT_APPROX");
+    return e != nullptr && atoi(e) != 0;
 }
 bool gradient_packed() {
     const char* e = getenv("FUGAL_GRAD_PACKED");
@@ -489,6 +503,8 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
                 gradient_kernel<true, 8, 6><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else if (minb == 8 && !gradient_packed())
                 gradient_kernel<true, 4, 8, false><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
+            else if (minb == 8 && gradient_sqrt_approx())
+                gradient_kernel<true, 4, 8, true, true><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else if (minb == 8)
                 gradient_kernel<true, 4, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
             else
