@@ -97,6 +97,13 @@ SIGNATURES = {
     "fugal_fw_gradient_column_stats": (_INT, [_I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _I64, _D, _D, _D, _P, _P,
                                               _P, _I64, _P, _SZ, _P, _I64, _P]),
     "fugal_fw_update": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _P]),
+    "fugal_fw_update_collect": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _P, _P, _INT,
+                                       _P, _P]),
+    "fugal_csr_edge_rows": (_INT, [_P, _I64, _I64, _P, _P]),
+    "fugal_structural_refresh": (_INT, [_I64, _P, _P, _P, _P, _P, _I64, _P, _I64, _INT, _P, _SZ, _P, _P]),
+    "fugal_structural_scatter": (_INT, [_I64, _P, _P, _I64, _P, _P, _P, _P, _INT, _D, _P, _I64, _P, _P]),
+    "fugal_fw_gradient_structural": (_INT, [_I64, _P, _I64, _D, _INT, _P, _I64, _P, _P, _P, _I64, _D, _D, _D, _P,
+                                            _P, _P, _I64, _P, _I64, _P]),
     "fugal_fw_direction": (_INT, [_I64, _P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _P, _I64, _P, _INT,
                                   _P]),
     "fugal_fw_line_search_update": (_INT, [_I64, _P, _I64, _P, _I64, _P, _I64, _D, _P, _P, _P, _P]),

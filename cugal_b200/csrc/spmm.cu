@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstdint>
 
@@ -360,6 +361,183 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
     }
 }
 
+// Fixed-point refresh of the structural term: the gather of gradient_kernel
+// (Y = B Tt = (A P B)^T over the tile), stored as Mq[i][j] = round(APB * scale)
+// in int64 (lane = j, so each store is a 256-byte row segment).  APB >= 0; a
+// value at or above 2^62 (or not finite) sets flags[1] and stores 0.
+template <int U = 4>
+__global__ void __launch_bounds__(kSpmmThreads) structural_refresh_kernel(const int* __restrict__ rp,
+                                                                          const int* __restrict__ col,
+                                                                          const float* __restrict__ Tt, long long ldt,
+                                                                          int n, long long* __restrict__ Mq,
+                                                                          long long ldm, double scale, int* flags) {
+    __shared__ Tile tile;
+    const int j0 = blockIdx.x * kTileRows;
+    const int i0 = blockIdx.y * kTileCols;
+    gather_tile<true, U>(rp, col, Tt, ldt, n, j0, i0, tile, 1.0f);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = j0 + lane;
+    if (j >= n) return;
+    bool bad = false;
+    for (int q = warp; q < kChunks; q += kSpmmThreads / 32) {
+        const int ib = i0 + 4 * q;
+        if (ib >= n) break;
+        const float4 a = tile.at(lane, q);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (ib + t >= n) break;
+            const double x = static_cast<double>(av[t]) * scale;
+            long long m = 0;
+            if (x < 4611686018427387904.0 && x >= 0.0) m = __double2ll_rn(x);
+            else bad = true;
+            Mq[row_offset(ib + t, ldm) + j] = m;
+        }
+    }
+    if (bad) atomicOr(&flags[1], 1);
+}
+
+// The gradient of gradient_kernel with APB read from the fixed-point structural
+// term (apb = (float)(Mq * m_scale)) instead of gathered: an elementwise pass.
+// CTA tile: 128 rows (i0 = 128 blockIdx.y, the column-statistics panel) x 128
+// columns (j0 = 128 blockIdx.x); lane l owns columns j0 + 4l .. j0 + 4l + 3 and
+// warp w the rows i0 + w + 8r, so every warp access is one contiguous row segment
+// (1 KB of Mq, 512 B of P and of out).  The per-column (max, sum) in base 2 is
+// kept online (one ex2 per element) and merged over the warps in shared memory.
+// SHIFT: Mq is also written back divided by 2^shift (rounded half up).
+constexpr int kStructThreads = 256;
+constexpr int kStructRows = 128;
+constexpr int kStructCols = 128;
+
+template <bool COLSTATS, bool SHIFT>
+__global__ void __launch_bounds__(kStructThreads) gradient_structural_kernel(long long* __restrict__ Mq,
+                                                                              long long ldm, double m_scale,
+                                                                              int shift, int n,
+                                                                              const EpilogueArgs ep) {
+    constexpr int kWarps = kStructThreads / 32;
+    __shared__ float2 cst[COLSTATS ? kWarps : 1][kStructCols];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j0 = blockIdx.x * kStructCols;
+    const int i0 = blockIdx.y * kStructRows;
+    const int jb = j0 + 4 * lane;
+    const bool has_f = ep.fs != nullptr;
+    const bool has_d = !has_f && ep.D != nullptr;
+    const float lam = static_cast<float>(ep.lam);
+    const bool use_p = lam != 0.f;
+    const bool full = jb + 3 < n;
+    float4 f2[4];
+    double vj[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int j = jb + c;
+        f2[c] = (has_f && j < n) ? reinterpret_cast<const float4*>(ep.ft)[j] : make_float4(0, 0, 0, 0);
+        vj[c] = (ep.V != nullptr && j < n) ? ep.V[j] : 0.0;
+    }
+    float cm[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    float cs[4] = {0.f, 0.f, 0.f, 0.f};
+    const long long half = SHIFT ? (1ll << (shift - 1)) : 0;
+    if (jb < n) {
+#pragma unroll 2
+        for (int r = 0; r < kStructRows / kWarps; ++r) {
+            const int i = i0 + warp + kWarps * r;
+            if (i >= n) break;
+            long long* mrow = Mq + row_offset(i, ldm) + jb;
+            long long m[4];
+            float p[4] = {0.f, 0.f, 0.f, 0.f};
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+            if (full) {
+                const longlong2 a = *reinterpret_cast<const longlong2*>(mrow);
+                const longlong2 b = *reinterpret_cast<const longlong2*>(mrow + 2);
+                m[0] = a.x; m[1] = a.y; m[2] = b.x; m[3] = b.y;
+                if (use_p) {
+                    const float4 p4 = *reinterpret_cast<const float4*>(ep.P + row_offset(i, ep.ldp) + jb);
+                    p[0] = p4.x; p[1] = p4.y; p[2] = p4.z; p[3] = p4.w;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    m[c] = jb + c < n ? mrow[c] : 0;
+                    if (use_p && jb + c < n) p[c] = ep.P[row_offset(i, ep.ldp) + jb + c];
+                }
+            }
+            if (has_d) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (jb + c < n) d[c] = ep.D[row_offset(i, ep.ldd) + jb + c];
+            }
+            const double ui = ep.U ? ep.U[i] : 0.0;
+            const float4 f1 = has_f ? reinterpret_cast<const float4*>(ep.fs)[i] : make_float4(0, 0, 0, 0);
+            float o[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float apb = __double2float_rn(__ll2double_rn(m[c]) * m_scale);
+                // the FP32 gradient in the order of gradient_kernel's scalar path
+                float reg = 0.f;
+                if (use_p) reg = __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, p[c])));
+                float g = __fadd_rn(__fmul_rn(-2.0f, apb), reg);
+                if (has_f) {
+                    const float d0 = __fsub_rn(f1.x, f2[c].x), d1 = __fsub_rn(f1.y, f2[c].y);
+                    const float d2 = __fsub_rn(f1.z, f2[c].z), d3 = __fsub_rn(f1.w, f2[c].w);
+                    g = __fadd_rn(g, __fsqrt_rn(__fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))))));
+                } else if (has_d) {
+                    g = __fadd_rn(g, d[c]);
+                }
+                o[c] = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + vj[c]));
+                if (COLSTATS && jb + c < n) {
+                    const float x = o[c] * kLog2e;
+                    if (x > cm[c]) {
+                        cs[c] = fmaf(cs[c], ex2(cm[c] - x), 1.0f);
+                        cm[c] = x;
+                    } else {
+                        cs[c] += ex2(x - cm[c]);
+                    }
+                }
+            }
+            float* orow = ep.out + row_offset(i, ep.ldo) + jb;
+            if (full) {
+                *reinterpret_cast<float4*>(orow) = make_float4(o[0], o[1], o[2], o[3]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (jb + c < n) orow[c] = o[c];
+            }
+            if constexpr (SHIFT) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) m[c] = (m[c] + half) >> shift;
+                if (full) {
+                    reinterpret_cast<longlong2*>(mrow)[0] = make_longlong2(m[0], m[1]);
+                    reinterpret_cast<longlong2*>(mrow)[1] = make_longlong2(m[2], m[3]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (jb + c < n) mrow[c] = m[c];
+                }
+            }
+        }
+    }
+    if constexpr (COLSTATS) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cst[warp][4 * lane + c] = make_float2(cm[c], cs[c]);
+        __syncthreads();
+        if (threadIdx.x < kStructCols && j0 + static_cast<int>(threadIdx.x) < n) {
+            const int t = threadIdx.x;
+            float M = -INFINITY;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) M = fmaxf(M, cst[w][t].x);
+            float S = 0.f;
+            if (M != -INFINITY) {
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w) {
+                    const float2 ps = cst[w][t];
+                    if (ps.x != -INFINITY) S += ps.y * ex2(ps.x - M);
+                }
+            }
+            ep.colpart[static_cast<size_t>(blockIdx.y) * ep.ldc + j0 + t] = make_float2(M, S);
+        }
+    }
+}
+
 // out^T[j][i] = sign * sum_{k in N(i)} Q[j][k]  (M = Q^T operand of the reference's adjacency_matmul)
 __global__ void spmm_transposed_operand_kernel(const int* __restrict__ rp, const int* __restrict__ col,
                                                const float* __restrict__ Q, long long ldq, int n,
@@ -549,4 +727,83 @@ extern "C" fugal_status fugal_fw_gradient_column_stats(
     return fw_gradient(n, a_row_pointers, a_col_indices, b_row_pointers, b_col_indices, P, ldp, source_features,
                        target_features, D, ldd, lambda, lambda_scale, out_scale, U, V, out, ldo, workspace,
                        workspace_bytes, column_partials, ldc, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" fugal_status fugal_structural_refresh(int64_t n, const int32_t* a_row_pointers,
+                                                 const int32_t* a_col_indices, const int32_t* b_row_pointers,
+                                                 const int32_t* b_col_indices, const float* P, int64_t ldp,
+                                                 int64_t* Mq, int64_t ldm, int32_t frac_bits, void* workspace,
+                                                 size_t workspace_bytes, int32_t* flags, fugal_stream_t stream_) {
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    const char* who = "fugal_structural_refresh";
+    FUGAL_TRY(check_csr(a_row_pointers, a_col_indices, n, who));
+    FUGAL_TRY(check_csr(b_row_pointers, b_col_indices, n, who));
+    if (P == nullptr || Mq == nullptr || workspace == nullptr || flags == nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "%s: null pointer", who);
+    if (ldp < n || (ldp % 4) != 0 || !aligned16(P) || ldm < n || ldp >= (1ll << 32) || ldm >= (1ll << 32))
+        return fail(FUGAL_BAD_SHAPE, "%s: P needs ld >= n, ld %% 4 == 0, 16-byte base; ldm >= n; ld < 2^32", who);
+    if (frac_bits < 0 || frac_bits > 60) return fail(FUGAL_BAD_ARGUMENT, "%s: frac_bits must be in [0, 60]", who);
+    size_t need = 0;
+    FUGAL_TRY(fugal_gradient_workspace_size(n, &need));
+    if (workspace_bytes < need || !aligned16(workspace))
+        return fail(FUGAL_WORKSPACE_TOO_SMALL, "%s: workspace %zu < %zu bytes", who, workspace_bytes, need);
+    float* Tt = static_cast<float*>(workspace);
+    const int64_t ldt = (n + 3) / 4 * 4;
+    dim3 grid(static_cast<unsigned>((n + kTileRows - 1) / kTileRows),
+              static_cast<unsigned>((n + kTileCols - 1) / kTileCols));
+    LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
+    spmm_kernel<true, 4><<<grid, kSpmmThreads, 0, stream>>>(a_row_pointers, a_col_indices, P, ldp,
+                                                             static_cast<int>(n), Tt, ldt, 1, 1.f);
+    FUGAL_TRY(launch_check("fugal_structural_refresh: A P"));
+    structural_refresh_kernel<4><<<grid, kSpmmThreads, 0, stream>>>(b_row_pointers, b_col_indices, Tt, ldt,
+                                                                     static_cast<int>(n),
+                                                                     reinterpret_cast<long long*>(Mq), ldm,
+                                                                     std::ldexp(1.0, frac_bits), flags);
+    return launch_check("fugal_structural_refresh: (A P) B");
+}
+
+extern "C" fugal_status fugal_fw_gradient_structural(int64_t n, int64_t* Mq_, int64_t ldm, double m_scale,
+                                                     int32_t shift, const float* P, int64_t ldp,
+                                                     const float* source_features, const float* target_features,
+                                                     const float* D, int64_t ldd, double lambda, double lambda_scale,
+                                                     double out_scale, const double* U, const double* V, float* out,
+                                                     int64_t ldo, float* column_partials, int64_t ldc,
+                                                     fugal_stream_t stream_) {
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+    const char* who = "fugal_fw_gradient_structural";
+    if (n <= 0 || n > (1ll << 30)) return fail(FUGAL_BAD_SHAPE, "%s: bad n", who);
+    if (Mq_ == nullptr || P == nullptr || out == nullptr) return fail(FUGAL_BAD_ARGUMENT, "%s: null pointer", who);
+    if ((source_features == nullptr) != (target_features == nullptr))
+        return fail(FUGAL_BAD_ARGUMENT, "%s: give both feature matrices or neither", who);
+    if ((U == nullptr) != (V == nullptr)) return fail(FUGAL_BAD_ARGUMENT, "%s: give both U and V", who);
+    if (source_features != nullptr && D != nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "%s: give features or a distance matrix, not both", who);
+    if (D != nullptr && ldd < n) return fail(FUGAL_BAD_SHAPE, "%s: ldd < n", who);
+    if (ldm < n || (ldm % 4) != 0 || !aligned16(Mq_))
+        return fail(FUGAL_BAD_SHAPE, "%s: Mq needs ld >= n, ld %% 4 == 0, 16-byte base", who);
+    if (ldp < n || (ldp % 4) != 0 || !aligned16(P) || ldo < n || (ldo % 4) != 0 || !aligned16(out))
+        return fail(FUGAL_BAD_SHAPE, "%s: P and out need ld >= n, ld %% 4 == 0, 16-byte base", who);
+    if (ldp >= (1ll << 32) || ldo >= (1ll << 32) || ldm >= (1ll << 32) || (D != nullptr && ldd >= (1ll << 32)))
+        return fail(FUGAL_BAD_SHAPE, "%s: ld >= 2^32", who);
+    if (source_features && (!aligned16(source_features) || !aligned16(target_features)))
+        return fail(FUGAL_BAD_SHAPE, "%s: feature rows must be 16-byte aligned", who);
+    if (column_partials != nullptr && (ldc < n || (reinterpret_cast<uintptr_t>(column_partials) & 7u) != 0))
+        return fail(FUGAL_BAD_SHAPE, "%s: partials need ldc >= n and 8-byte alignment", who);
+    if (shift < 0 || shift > 62) return fail(FUGAL_BAD_ARGUMENT, "%s: shift must be in [0, 62]", who);
+    EpilogueArgs ep{P,   ldp, source_features, target_features, D, ldd, lambda * lambda_scale, out_scale, U, V, out,
+                    ldo, reinterpret_cast<float2*>(column_partials), ldc};
+    dim3 grid(static_cast<unsigned>((n + kStructCols - 1) / kStructCols),
+              static_cast<unsigned>((n + kStructRows - 1) / kStructRows));
+    const int ni = static_cast<int>(n);
+    long long* Mq = reinterpret_cast<long long*>(Mq_);
+    LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
+    if (column_partials != nullptr && shift > 0)
+        gradient_structural_kernel<true, true><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, shift, ni, ep);
+    else if (column_partials != nullptr)
+        gradient_structural_kernel<true, false><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, 0, ni, ep);
+    else if (shift > 0)
+        gradient_structural_kernel<false, true><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, shift, ni, ep);
+    else
+        gradient_structural_kernel<false, false><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, 0, ni, ep);
+    return launch_check(who);
 }

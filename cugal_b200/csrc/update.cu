@@ -25,26 +25,57 @@ inline dim3 ew_grid(int64_t n) {
     return dim3(static_cast<unsigned>(n), static_cast<unsigned>((n + kEwThreads * 4 - 1) / (kEwThreads * 4)));
 }
 
+// Where the update records the plan's nonzero entries (fugal_fw_update_collect):
+// per row k, counts[k] entries (column, q) at entries[k * slots ...] in no
+// particular order; flags[0] is set when a row has more than `slots` of them or
+// their sum exceeds FUGAL_PLAN_ROW_SUM_MAX.
+struct PlanOut {
+    int* counts;
+    fugal_plan_entry* entries;
+    int slots;
+    int* flags;
+};
+
 // q = exp(L + u_i + v_j); P += alpha (q - P); gap += (q - P) * (-reg (L - U_i - V_j)).
-// Grid-stride over (row, 1024-column chunk) units, each thread one float4 of a
-// unit per step; every block reduces its gap once at the end (one FP64 atomic
-// per block instead of one per unit).
+// Rows grid-strided over the blocks, each row's columns in chunks of 1024 (one
+// float4 per thread per chunk); every block reduces its gap once at the end (one
+// FP64 atomic per block).  EMIT: the block also appends each q > 0 of the row to
+// the row's plan slots (shared-memory counter, two barriers per row).
+template <bool EMIT>
 __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict__ P, long long ldp,
                                                                const float* __restrict__ L, long long ldl,
                                                                const float* __restrict__ u,
                                                                const float* __restrict__ v,
                                                                const double* __restrict__ U,
                                                                const double* __restrict__ V, int n, float alpha,
-                                                               double reg, double* gap) {
+                                                               double reg, double* gap, PlanOut plan) {
     __shared__ double red[32];
+    __shared__ int s_count;
+    __shared__ float s_sum;
     constexpr int kChunk = kEwThreads * 4;
     double g = 0.0;
-    // rows grid-strided, each row's columns in chunks of kChunk (no division per chunk)
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
+      if constexpr (EMIT) {
+          if (threadIdx.x == 0) {
+              s_count = 0;
+              s_sum = 0.f;
+          }
+          __syncthreads();
+      }
       const float ui = u[i];
       const double Ui = U ? U[i] : 0.0;
       float* prow = P + static_cast<size_t>(i) * ldp;
       const float* lrow = L + static_cast<size_t>(i) * ldl;
+      fugal_plan_entry* slots = EMIT ? plan.entries + static_cast<size_t>(i) * plan.slots : nullptr;
+      auto record = [&](int j, float qv) {
+          if constexpr (EMIT) {
+              if (qv > 0.f) {
+                  const int s = atomicAdd(&s_count, 1);
+                  atomicAdd(&s_sum, qv);
+                  if (s < plan.slots) slots[s] = fugal_plan_entry{j, qv};
+              }
+          }
+      };
       for (int j0 = threadIdx.x * 4; j0 < n; j0 += kChunk) {
         if (j0 + 4 <= n) {
             const float4 l4 = *reinterpret_cast<const float4*>(lrow + j0);
@@ -55,21 +86,32 @@ __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict
             float pv[4] = {p4.x, p4.y, p4.z, p4.w};
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const float diff = expf(lv[q] + ui + vv[q]) - pv[q];
+                const float qv = expf(lv[q] + ui + vv[q]);
+                const float diff = qv - pv[q];
                 const double C = -reg * (static_cast<double>(lv[q]) - Ui - (V ? V[j0 + q] : 0.0));
                 g += static_cast<double>(diff) * C;
                 pv[q] = fmaf(alpha, diff, pv[q]);
+                record(j0 + q, qv);
             }
             p4 = make_float4(pv[0], pv[1], pv[2], pv[3]);
             *reinterpret_cast<float4*>(prow + j0) = p4;
         } else {
             for (int j = j0; j < n; ++j) {
-                const float diff = expf(lrow[j] + ui + v[j]) - prow[j];
+                const float qv = expf(lrow[j] + ui + v[j]);
+                const float diff = qv - prow[j];
                 const double C = -reg * (static_cast<double>(lrow[j]) - Ui - (V ? V[j] : 0.0));
                 g += static_cast<double>(diff) * C;
                 prow[j] = fmaf(alpha, diff, prow[j]);
+                record(j, qv);
             }
         }
+      }
+      if constexpr (EMIT) {
+          __syncthreads();
+          if (threadIdx.x == 0) {
+              plan.counts[i] = s_count;
+              if (s_count > plan.slots || !(s_sum <= FUGAL_PLAN_ROW_SUM_MAX)) atomicOr(plan.flags, 1);
+          }
       }
     }
     g = block_sum(g, red);
@@ -207,11 +249,11 @@ fugal_status check_square(const void* p, int64_t ld, int64_t n, const char* who,
 
 using namespace fugal;
 
-extern "C" fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32,
-                                        const float* u, const float* v, double* U, double* V, double alpha,
-                                        double regularization, double* gap, int commit, fugal_stream_t stream_) {
-    cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
-    const char* who = "fugal_fw_update";
+namespace {
+
+fugal_status fw_update(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32, const float* u,
+                       const float* v, double* U, double* V, double alpha, double regularization, double* gap,
+                       int commit, const PlanOut* plan, const char* who, cudaStream_t stream) {
     FUGAL_TRY(check_square(P, ldp, n, who, "P"));
     FUGAL_TRY(check_square(cost32, ld32, n, who, "cost32"));
     if (u == nullptr || v == nullptr || gap == nullptr) return fail(FUGAL_BAD_ARGUMENT, "%s: null duals or gap", who);
@@ -219,12 +261,19 @@ extern "C" fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const 
     if (commit && U == nullptr) return fail(FUGAL_BAD_ARGUMENT, "%s: commit needs U and V", who);
     if ((ldp % 4) || (ld32 % 4) || !aligned16(P) || !aligned16(cost32) || !aligned16(v))
         return fail(FUGAL_BAD_SHAPE, "%s: P, cost32, v need 16-byte rows", who);
-    FUGAL_TRY(cuda_check(cudaMemsetAsync(gap, 0, sizeof(double), stream), "fugal_fw_update: clear gap"));
+    FUGAL_TRY(cuda_check(cudaMemsetAsync(gap, 0, sizeof(double), stream), who));
     {
         LaunchScope scope(FUGAL_KERNEL_UPDATE, stream);
         const int blocks = static_cast<int>(std::min<int64_t>(n, static_cast<int64_t>(sm_count()) * 8));
-        fw_update_kernel<<<blocks, kEwThreads, 0, stream>>>(P, ldp, cost32, ld32, u, v, U, V, static_cast<int>(n),
-                                                            static_cast<float>(alpha), regularization, gap);
+        if (plan != nullptr)
+            fw_update_kernel<true><<<blocks, kEwThreads, 0, stream>>>(P, ldp, cost32, ld32, u, v, U, V,
+                                                                      static_cast<int>(n), static_cast<float>(alpha),
+                                                                      regularization, gap, *plan);
+        else
+            fw_update_kernel<false><<<blocks, kEwThreads, 0, stream>>>(P, ldp, cost32, ld32, u, v, U, V,
+                                                                       static_cast<int>(n),
+                                                                       static_cast<float>(alpha), regularization,
+                                                                       gap, PlanOut{});
         FUGAL_TRY(launch_check(who));
     }
     if (commit) {
@@ -234,6 +283,29 @@ extern "C" fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const 
         FUGAL_TRY(launch_check("fugal_fw_update: commit"));
     }
     return FUGAL_OK;
+}
+
+}  // namespace
+
+extern "C" fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32,
+                                        const float* u, const float* v, double* U, double* V, double alpha,
+                                        double regularization, double* gap, int commit, fugal_stream_t stream) {
+    return fw_update(n, P, ldp, cost32, ld32, u, v, U, V, alpha, regularization, gap, commit, nullptr,
+                     "fugal_fw_update", reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" fugal_status fugal_fw_update_collect(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32,
+                                                const float* u, const float* v, double* U, double* V, double alpha,
+                                                double regularization, double* gap, int commit, int32_t* plan_counts,
+                                                fugal_plan_entry* plan_entries, int32_t slots, int32_t* flags,
+                                                fugal_stream_t stream) {
+    const char* who = "fugal_fw_update_collect";
+    if (plan_counts == nullptr || plan_entries == nullptr || flags == nullptr)
+        return fail(FUGAL_BAD_ARGUMENT, "%s: null plan buffers", who);
+    if (slots < 1 || slots > 1024) return fail(FUGAL_BAD_ARGUMENT, "%s: slots must be in [1, 1024]", who);
+    const PlanOut plan{plan_counts, plan_entries, slots, flags};
+    return fw_update(n, P, ldp, cost32, ld32, u, v, U, V, alpha, regularization, gap, commit, &plan, who,
+                     reinterpret_cast<cudaStream_t>(stream));
 }
 
 extern "C" fugal_status fugal_update_quasi_permutation_log(float* P, int64_t ldp, const float* K, int64_t ldk,

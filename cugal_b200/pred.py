@@ -5,16 +5,23 @@ return value ``(P as a host numpy array, [(i, column_i)])``.  The Frank-Wolfe
 loop (``pred.py:89-148``) runs as three kernel-library calls per step, all
 asynchronous on the current CUDA stream:
 
-  gradient  ``fugal_fw_gradient_column_stats``  -2 A P B + D + lambda (1 - 2P), written
+  gradient  ``fugal_fw_gradient_structural``  -2 A P B + D + lambda (1 - 2P), written
                                       as the absorbed Sinkhorn input K + U_i + V_j, and the
-                                      solve's first column update
+                                      solve's first column update, with A P B read from the
+                                      term kept across steps (structural.py); the two-SpMM
+                                      ``fugal_fw_gradient_column_stats`` when that term is
+                                      off or has to be recomputed
   solve     ``fugal_sinkhorn_solve``  whole log-domain solve, decisions on device
-  update    ``fugal_fw_update``       P += alpha (q - P), FP64 duality gap, duals folded
-            (``fugal_fw_direction`` + ``fugal_fw_line_search_update`` with line_search)
+  update    ``fugal_fw_update_collect``  P += alpha (q - P), FP64 duality gap, duals folded,
+                                      the plan's nonzero entries recorded; then
+                                      ``fugal_structural_scatter`` adds alpha A q B
+            (``fugal_fw_direction`` + ``fugal_fw_line_search_update`` with line_search,
+            which keeps the two-SpMM gradient)
 
-The host only waits inside a solve (to stop enqueuing sweeps after
-convergence) and, when ``frank_wolfe_threshold`` is set, for the gap.  Only
-CUDA devices are supported; a CPU config raises.
+The host waits inside a solve (to stop enqueuing sweeps after convergence),
+once per gradient for the kept term's two flags, and, when
+``frank_wolfe_threshold`` is set, for the gap.  Only CUDA devices are
+supported; a CPU config raises.
 """
 
 from __future__ import annotations
@@ -36,6 +43,7 @@ from .exact_lap import FUGAL_ITER_LIMIT, FUGAL_OK, default_max_steps, exact_assi
 from .greedy_lap import greedy_assign
 from .profile import Phase, Profile, SinkhornProfile, TimeStamp
 from .sinkhorn import SinkhornSolver, StandardSolver, exp_scale, padded_ld, read_record
+from .structural import StructuralTerm, enabled_by_default as structural_enabled_by_default
 
 
 def check_config(config: Config) -> None:
@@ -117,6 +125,10 @@ class FrankWolfeEngine:
             self.D = self.features.float().contiguous()
         # dense reference path adds the lambda term twice (cugal/pred.py:46-50)
         self.lambda_scale = 1.0 if self.config.use_sparse_adjacency else 2.0
+        # A P B kept across steps (structural.py), made at the first gradient that uses it
+        self.structural: StructuralTerm | None = None
+        self._structural_on = (not self.standard and not self.config.line_search
+                               and structural_enabled_by_default())
 
     @property
     def P(self) -> torch.Tensor:
@@ -132,6 +144,20 @@ class FrankWolfeEngine:
         to_cost = out is None
         out = self.cost32 if out is None else out
         scale = (-1.0 / reg) if out_scale is None else out_scale
+        if to_cost and absorbed and out_scale is None and not self.standard:
+            st = self._structural_term()
+            if st is not None and st.prepare(self.P_buf):
+                # the Sinkhorn input from the kept A P B (one elementwise pass)
+                k = st.fixed.shift()
+                N.call("fugal_fw_gradient_structural", self.n, st.Mq.data_ptr(), self.ld, st.fixed.m_scale(), k,
+                       self.P_buf.data_ptr(), self.ld, N.ptr(self.fs), N.ptr(self.ft), N.ptr(self.D),
+                       self.n if self.D is not None else 0, float(lam), self.lambda_scale, scale, N.ptr(self.U),
+                       N.ptr(self.V), out.data_ptr(), N.matrix_ld(out, "out"), self.colpart.data_ptr(), self.ld,
+                       N.stream_handle(self.device))
+                if k:
+                    st.fixed.shifted(k)
+                self.colpart_valid = True
+                return out
         args = (self.n, self.A.row_pointers.data_ptr(), self.A.col_indices.data_ptr(),
                 self.B.row_pointers.data_ptr(), self.B.col_indices.data_ptr(), self.P_buf.data_ptr(), self.ld,
                 N.ptr(self.fs), N.ptr(self.ft), N.ptr(self.D), self.n if self.D is not None else 0,
@@ -173,10 +199,27 @@ class FrankWolfeEngine:
                    self.u.data_ptr(), self.v.data_ptr(), self.cost32.data_ptr(), self.ld, float(alpha),
                    self.gap.data_ptr(), N.stream_handle(self.device))
             return self.gap
+        st = self.structural
+        if st is not None and st.valid:
+            st.collect_update(self.P_buf, self.cost32, self.u, self.v, self.U, self.V, float(alpha),
+                              float(self.config.sinkhorn_regularization), self.gap)
+            return self.gap
         N.call("fugal_fw_update", self.n, self.P_buf.data_ptr(), self.ld, self.cost32.data_ptr(), self.ld,
                self.u.data_ptr(), self.v.data_ptr(), self.U.data_ptr(), self.V.data_ptr(), float(alpha),
                float(self.config.sinkhorn_regularization), self.gap.data_ptr(), 1, N.stream_handle(self.device))
+        if st is not None:
+            st.invalidate()
         return self.gap
+
+    def _structural_term(self) -> StructuralTerm | None:
+        """The kept A P B, allocated on first use (8 bytes per entry of P); None
+        when switched off or when its buffers do not fit."""
+        if self.structural is None and self._structural_on:
+            try:
+                self.structural = StructuralTerm(self.A, self.B, self.n, self.ld, self.device, self.grad_ws)
+            except (torch.OutOfMemoryError, ValueError):
+                self._structural_on = False
+        return self.structural
 
     def _line_search_update(self, lam: float) -> torch.Tensor:
         k = self.updates - 1

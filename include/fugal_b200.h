@@ -363,6 +363,75 @@ fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const float* cost
                              const float* u, const float* v, double* U, double* V, double alpha,
                              double regularization, double* gap, int commit, fugal_stream_t stream);
 
+/* ============ structural term kept across Frank-Wolfe steps ==============
+ * No counterpart in the reference, which forms -A P B from scratch with two
+ * SpMMs every step (cugal/pred.py:54-74).  With the fixed step of
+ * cugal/pred.py:133-141, P' = (1 - alpha) P + alpha q, so M = A P B follows
+ *   M' = (1 - alpha) M + alpha A q B,
+ * and once the Sinkhorn plan q has few nonzero entries per row (one per row
+ * for a converged solve at small regularization) A q B is a sparse product.
+ * The gradient then reads a stored M instead of gathering P through A and B.
+ *
+ * M is kept as int64 fixed point: M[i][j] = Mq[i][j] * 2^-frac_bits * scale,
+ * with scale (the product of the (1 - alpha) factors since the last refresh)
+ * and frac_bits held by the caller.  A step only adds to the entries that A q B
+ * touches; integer addition is associative, so the sums do not depend on the
+ * order of the atomic adds and reruns are bit-identical.  Choose frac_bits so
+ * that d_max * FUGAL_PLAN_ROW_SUM_MAX * 2^frac_bits / scale < 2^62, d_max the
+ * largest degree of A, for every scale used between refreshes.
+ *
+ * flags: two device int32, zeroed by the caller.  flags[0] != 0: an update
+ * (fugal_fw_update_collect) met a plan row with more than `slots` nonzero
+ * entries or a row sum above FUGAL_PLAN_ROW_SUM_MAX; the scatter is skipped
+ * and Mq is stale until the next refresh.  flags[1] != 0: a refresh met a
+ * value outside the fixed-point range (Mq unusable). */
+#define FUGAL_PLAN_ROW_SUM_MAX 32.0f
+typedef struct {
+    int32_t column;
+    float value;
+} fugal_plan_entry;
+
+/* rows[e] = the row of edge e of an n-row CSR matrix, e < nnz = row_pointers[n]. */
+fugal_status fugal_csr_edge_rows(const int32_t* row_pointers, int64_t n, int64_t nnz, int32_t* rows,
+                                 fugal_stream_t stream);
+
+/* Mq[i][j] = round((A P B)[i][j] * 2^frac_bits) for i, j < n (the SpMM pair of
+ * fugal_fw_gradient, same workspace); flags[1] is set on a value >= 2^62. */
+fugal_status fugal_structural_refresh(int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices,
+                                      const int32_t* b_row_pointers, const int32_t* b_col_indices, const float* P,
+                                      int64_t ldp, int64_t* Mq, int64_t ldm, int32_t frac_bits, void* workspace,
+                                      size_t workspace_bytes, int32_t* flags, fugal_stream_t stream);
+
+/* fugal_fw_update that also records the plan's nonzero entries: for each row k,
+ * plan_counts[k] = the number of j with q_kj > 0, and the first min(count, slots)
+ * of them as (j, q_kj) at plan_entries[k * slots ...], in no particular order. */
+fugal_status fugal_fw_update_collect(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32,
+                                     const float* u, const float* v, double* U, double* V, double alpha,
+                                     double regularization, double* gap, int commit, int32_t* plan_counts,
+                                     fugal_plan_entry* plan_entries, int32_t slots, int32_t* flags,
+                                     fugal_stream_t stream);
+
+/* Mq[i][j] += round(q_kl * increment_scale) for every recorded plan entry
+ * (k, l, q_kl), i in N_A(k), j in N_B(l) (A, B symmetric, so this adds
+ * round(increment_scale q) through A q B); a_edge_rows from fugal_csr_edge_rows
+ * on A, a_nnz its edge count.  Does nothing when flags[0] or flags[1] is set. */
+fugal_status fugal_structural_scatter(int64_t n, const int32_t* a_col_indices, const int32_t* a_edge_rows,
+                                      int64_t a_nnz, const int32_t* b_row_pointers,
+                                      const int32_t* b_col_indices, const int32_t* plan_counts,
+                                      const fugal_plan_entry* plan_entries, int32_t slots, double increment_scale,
+                                      int64_t* Mq, int64_t ldm, const int32_t* flags, fugal_stream_t stream);
+
+/* The gradient of fugal_fw_gradient (column_partials != NULL: of
+ * fugal_fw_gradient_column_stats) with (A P B)[i][j] = (float)(Mq[i][j] * m_scale)
+ * in place of the SpMM pair.  shift > 0 also rescales Mq in place by 2^-shift
+ * (rounded), for the caller to multiply its scale by 2^shift. */
+fugal_status fugal_fw_gradient_structural(int64_t n, int64_t* Mq, int64_t ldm, double m_scale, int32_t shift,
+                                          const float* P, int64_t ldp, const float* source_features,
+                                          const float* target_features, const float* D, int64_t ldd,
+                                          double lambda, double lambda_scale, double out_scale, const double* U,
+                                          const double* V, float* out, int64_t ldo, float* column_partials,
+                                          int64_t ldc, fugal_stream_t stream);
+
 /* Exact line search, opt-in (Config.line_search).  No counterpart in the
  * reference, which steps with alpha = 2/(2+it) (cugal/pred.py:133-141).  On the
  * objective f(P) = -<P, A P B> + <D, P> + lam' <P, 1 - P>, whose gradient is the
