@@ -98,7 +98,7 @@ SIGNATURES = {
                                               _P, _I64, _P, _SZ, _P, _I64, _P]),
     "fugal_fw_update": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _P]),
     "fugal_fw_update_collect": (_INT, [_I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _D, _D, _P, _INT, _P, _P, _INT,
-                                       _P, _P]),
+                                       _P]),
     "fugal_csr_edge_rows": (_INT, [_P, _I64, _I64, _P, _P]),
     "fugal_structural_refresh": (_INT, [_I64, _P, _P, _P, _P, _P, _I64, _P, _I64, _INT, _P, _SZ, _P, _P]),
     "fugal_structural_scatter": (_INT, [_I64, _P, _P, _I64, _P, _P, _P, _P, _INT, _D, _P, _I64, _P, _P]),

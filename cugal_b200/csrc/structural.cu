@@ -42,18 +42,26 @@ __global__ void csr_edge_rows_kernel(const int* __restrict__ rp, int n, int* __r
 __global__ void __launch_bounds__(kScatterThreads) structural_scatter_kernel(
     const int* __restrict__ a_col, const int* __restrict__ a_rows, long long nnz_a, const int* __restrict__ b_rp,
     const int* __restrict__ b_col, const int* __restrict__ counts, const fugal_plan_entry* __restrict__ entries,
-    int slots, double inc_scale, unsigned long long* __restrict__ Mq, long long ldm, const int* __restrict__ flags) {
-    if (flags[0] != 0 || flags[1] != 0) return;  // stale plan: the next gradient refreshes Mq
+    int slots, double inc_scale, unsigned long long* __restrict__ Mq, long long ldm, int* flags) {
+    if (flags[0] != 0 || flags[1] != 0) return;  // stale term: the next gradient refreshes Mq
     const int lane = threadIdx.x & 31;
     const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
     for (long long e = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); e < nnz_a;
          e += warps) {
         const int k = a_rows[e];
         const int i = a_col[e];
-        const int cnt = min(counts[k], slots);
+        const int cnt = counts[k];
+        const fugal_plan_entry* ent = entries + static_cast<size_t>(k) * slots;
+        // a row this step cannot add exactly: flag it (the next gradient recomputes Mq)
+        float rsum = 0.f;
+        for (int s = lane; s < min(cnt, slots); s += 32) rsum += ent[s].value;
+        rsum = warp_sum(rsum);
+        if (cnt > slots || !(rsum <= FUGAL_PLAN_ROW_SUM_MAX)) {
+            if (lane == 0) atomicOr(flags, 1);
+            continue;
+        }
         unsigned long long* mrow = Mq + static_cast<unsigned long long>(static_cast<unsigned>(i)) *
                                             static_cast<unsigned long long>(ldm);
-        const fugal_plan_entry* ent = entries + static_cast<size_t>(k) * slots;
         for (int s = 0; s < cnt; ++s) {
             const fugal_plan_entry pe = ent[s];
             const unsigned long long inc =
@@ -106,6 +114,6 @@ extern "C" fugal_status fugal_structural_scatter(int64_t n, const int32_t* a_col
                                                           static_cast<int64_t>(sm_count()) * 16));
     structural_scatter_kernel<<<blocks, kScatterThreads, 0, stream>>>(
         a_col_indices, a_edge_rows, a_nnz, b_row_pointers, b_col_indices, plan_counts, plan_entries, slots,
-        increment_scale, reinterpret_cast<unsigned long long*>(Mq), ldm, flags);
+        increment_scale, reinterpret_cast<unsigned long long*>(Mq), ldm, const_cast<int32_t*>(flags));
     return launch_check(who);
 }

@@ -27,20 +27,19 @@ inline dim3 ew_grid(int64_t n) {
 
 // Where the update records the plan's nonzero entries (fugal_fw_update_collect):
 // per row k, counts[k] entries (column, q) at entries[k * slots ...] in no
-// particular order; flags[0] is set when a row has more than `slots` of them or
-// their sum exceeds FUGAL_PLAN_ROW_SUM_MAX.
+// particular order (counts zeroed before the kernel; entries past `slots` are
+// counted, not stored; the scatter checks counts and row sums).
 struct PlanOut {
     int* counts;
     fugal_plan_entry* entries;
     int slots;
-    int* flags;
 };
 
 // q = exp(L + u_i + v_j); P += alpha (q - P); gap += (q - P) * (-reg (L - U_i - V_j)).
 // Rows grid-strided over the blocks, each row's columns in chunks of 1024 (one
 // float4 per thread per chunk); every block reduces its gap once at the end (one
-// FP64 atomic per block).  EMIT: the block also appends each q > 0 of the row to
-// the row's plan slots (shared-memory counter, two barriers per row).
+// FP64 atomic per block).  EMIT: each q > 0 also takes a slot of its row through
+// a global atomic on the row's count (a few per row, no barrier).
 template <bool EMIT>
 __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict__ P, long long ldp,
                                                                const float* __restrict__ L, long long ldl,
@@ -50,28 +49,18 @@ __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict
                                                                const double* __restrict__ V, int n, float alpha,
                                                                double reg, double* gap, PlanOut plan) {
     __shared__ double red[32];
-    __shared__ int s_count;
-    __shared__ float s_sum;
     constexpr int kChunk = kEwThreads * 4;
     double g = 0.0;
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
-      if constexpr (EMIT) {
-          if (threadIdx.x == 0) {
-              s_count = 0;
-              s_sum = 0.f;
-          }
-          __syncthreads();
-      }
       const float ui = u[i];
       const double Ui = U ? U[i] : 0.0;
       float* prow = P + static_cast<size_t>(i) * ldp;
-      const float* lrow = L + static_cast<size_t>(i) * ldl;
+    const float* lrow = L + static_cast<size_t>(i) * ldl;
       fugal_plan_entry* slots = EMIT ? plan.entries + static_cast<size_t>(i) * plan.slots : nullptr;
       auto record = [&](int j, float qv) {
           if constexpr (EMIT) {
               if (qv > 0.f) {
-                  const int s = atomicAdd(&s_count, 1);
-                  atomicAdd(&s_sum, qv);
+                  const int s = atomicAdd(&plan.counts[i], 1);
                   if (s < plan.slots) slots[s] = fugal_plan_entry{j, qv};
               }
           }
@@ -105,13 +94,6 @@ __global__ void __launch_bounds__(kEwThreads) fw_update_kernel(float* __restrict
                 record(j, qv);
             }
         }
-      }
-      if constexpr (EMIT) {
-          __syncthreads();
-          if (threadIdx.x == 0) {
-              plan.counts[i] = s_count;
-              if (s_count > plan.slots || !(s_sum <= FUGAL_PLAN_ROW_SUM_MAX)) atomicOr(plan.flags, 1);
-          }
       }
     }
     g = block_sum(g, red);
@@ -297,13 +279,16 @@ extern "C" fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const 
 extern "C" fugal_status fugal_fw_update_collect(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32,
                                                 const float* u, const float* v, double* U, double* V, double alpha,
                                                 double regularization, double* gap, int commit, int32_t* plan_counts,
-                                                fugal_plan_entry* plan_entries, int32_t slots, int32_t* flags,
+                                                fugal_plan_entry* plan_entries, int32_t slots,
                                                 fugal_stream_t stream) {
     const char* who = "fugal_fw_update_collect";
-    if (plan_counts == nullptr || plan_entries == nullptr || flags == nullptr)
+    if (plan_counts == nullptr || plan_entries == nullptr)
         return fail(FUGAL_BAD_ARGUMENT, "%s: null plan buffers", who);
     if (slots < 1 || slots > 1024) return fail(FUGAL_BAD_ARGUMENT, "%s: slots must be in [1, 1024]", who);
-    const PlanOut plan{plan_counts, plan_entries, slots, flags};
+    FUGAL_TRY(cuda_check(cudaMemsetAsync(plan_counts, 0, static_cast<size_t>(n) * sizeof(int32_t),
+                                         reinterpret_cast<cudaStream_t>(stream)),
+                         who));
+    const PlanOut plan{plan_counts, plan_entries, slots};
     return fw_update(n, P, ldp, cost32, ld32, u, v, U, V, alpha, regularization, gap, commit, &plan, who,
                      reinterpret_cast<cudaStream_t>(stream));
 }

@@ -17,9 +17,9 @@ gradient then becomes an elementwise pass over a stored ``M``
 ``(1 - a)`` factors go into the host-held ``scale``, so a step only adds to the
 entries ``A q B`` touches, and integer adds make the sums independent of the
 order of the device's atomics (reruns are bit-identical).  The update records
-the plan's nonzero entries per row (``fugal_fw_update_collect``); a row with
-more than ``SLOTS`` of them, or a plan row sum above ``ROW_SUM_MAX``, flags the
-step, and the next gradient recomputes ``Mq`` with the two SpMMs
+the plan's nonzero entries per row (``fugal_fw_update_collect``); the scatter
+flags a row with more than ``SLOTS`` of them, or a plan row sum above
+``ROW_SUM_MAX``, and the next gradient recomputes ``Mq`` with the two SpMMs
 (``fugal_structural_refresh``).  Nothing is dropped: every nonzero FP32 entry
 of ``q`` is either added exactly (to 2^-frac_bits) or the term is recomputed.
 
@@ -175,7 +175,7 @@ class StructuralTerm:
         stream = N.stream_handle(self.device)
         N.call("fugal_fw_update_collect", self.n, P_buf.data_ptr(), self.ld, cost32.data_ptr(), self.ld, u.data_ptr(),
                v.data_ptr(), U.data_ptr(), V.data_ptr(), float(alpha), float(reg), gap.data_ptr(), commit,
-               self.counts.data_ptr(), self.entries.data_ptr(), SLOTS, self.flags.data_ptr(), stream)
+               self.counts.data_ptr(), self.entries.data_ptr(), SLOTS, stream)
         factor = self.fixed.step(alpha)
         if factor is None:
             self.valid = False

@@ -380,11 +380,11 @@ fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const float* cost
  * that d_max * FUGAL_PLAN_ROW_SUM_MAX * 2^frac_bits / scale < 2^62, d_max the
  * largest degree of A, for every scale used between refreshes.
  *
- * flags: two device int32, zeroed by the caller.  flags[0] != 0: an update
- * (fugal_fw_update_collect) met a plan row with more than `slots` nonzero
- * entries or a row sum above FUGAL_PLAN_ROW_SUM_MAX; the scatter is skipped
- * and Mq is stale until the next refresh.  flags[1] != 0: a refresh met a
- * value outside the fixed-point range (Mq unusable). */
+ * flags: two device int32, zeroed by the caller.  flags[0] != 0: the scatter
+ * met a plan row with more than `slots` nonzero entries or a row sum above
+ * FUGAL_PLAN_ROW_SUM_MAX (that row is not added: Mq is stale until the next
+ * refresh).  flags[1] != 0: a refresh met a value outside the fixed-point range
+ * (Mq unusable). */
 #define FUGAL_PLAN_ROW_SUM_MAX 32.0f
 typedef struct {
     int32_t column;
@@ -403,18 +403,19 @@ fugal_status fugal_structural_refresh(int64_t n, const int32_t* a_row_pointers, 
                                       size_t workspace_bytes, int32_t* flags, fugal_stream_t stream);
 
 /* fugal_fw_update that also records the plan's nonzero entries: for each row k,
- * plan_counts[k] = the number of j with q_kj > 0, and the first min(count, slots)
- * of them as (j, q_kj) at plan_entries[k * slots ...], in no particular order. */
+ * plan_counts[k] = the number of j with q_kj > 0, and min(count, slots) of them
+ * as (j, q_kj) at plan_entries[k * slots ...], in no particular order. */
 fugal_status fugal_fw_update_collect(int64_t n, float* P, int64_t ldp, const float* cost32, int64_t ld32,
                                      const float* u, const float* v, double* U, double* V, double alpha,
                                      double regularization, double* gap, int commit, int32_t* plan_counts,
-                                     fugal_plan_entry* plan_entries, int32_t slots, int32_t* flags,
-                                     fugal_stream_t stream);
+                                     fugal_plan_entry* plan_entries, int32_t slots, fugal_stream_t stream);
 
 /* Mq[i][j] += round(q_kl * increment_scale) for every recorded plan entry
  * (k, l, q_kl), i in N_A(k), j in N_B(l) (A, B symmetric, so this adds
  * round(increment_scale q) through A q B); a_edge_rows from fugal_csr_edge_rows
- * on A, a_nnz its edge count.  Does nothing when flags[0] or flags[1] is set. */
+ * on A, a_nnz its edge count.  Does nothing when flags[0] or flags[1] is set on
+ * entry; sets flags[0] (and skips the row) for a row whose count exceeds slots
+ * or whose entries sum above FUGAL_PLAN_ROW_SUM_MAX. */
 fugal_status fugal_structural_scatter(int64_t n, const int32_t* a_col_indices, const int32_t* a_edge_rows,
                                       int64_t a_nnz, const int32_t* b_row_pointers,
                                       const int32_t* b_col_indices, const int32_t* plan_counts,
