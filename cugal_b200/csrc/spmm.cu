@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstdint>
+#include <type_traits>
 
 #include "fugal_common.cuh"
 #include "fugal_host.h"
@@ -200,9 +201,9 @@ struct EpilogueArgs {
 // FP32 arithmetic of two columns per FP32x2 instruction (the same IEEE operations
 // in the same order, so the same results) and the row duals read from shared
 // memory; other chunks take the scalar path.
-// SQ (packed path only): the distance's square root as sqrt.approx, the form the
-// reference's distance kernel is built with (--use_fast_math,
-// cuda_kernels/setup.py:19), instead of the IEEE-rounded one.
+// SQ: the distance's square root as sqrt.approx, the form the reference's
+// distance kernel is built with (--use_fast_math, cuda_kernels/setup.py:19),
+// instead of the IEEE-rounded one.
 template <bool COLSTATS, int U = 4, int MINB = 6, bool PK = true, bool SQ = false>
 __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int* __restrict__ rp,
                                                                 const int* __restrict__ col,
@@ -312,7 +313,11 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
                 const float4 f1 = fi[ii];
                 const float d0 = __fsub_rn(f1.x, f2.x), d1 = __fsub_rn(f1.y, f2.y);
                 const float d2 = __fsub_rn(f1.z, f2.z), d3 = __fsub_rn(f1.w, f2.w);
-                g = __fadd_rn(g, __fsqrt_rn(__fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))))));
+                const float ss = __fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))));
+                float dist;
+                if constexpr (SQ) asm("sqrt.approx.f32 %0, %1;" : "=f"(dist) : "f"(ss));
+                else dist = __fsqrt_rn(ss);
+                g = __fadd_rn(g, dist);
             } else if (ep.D != nullptr) {
                 g = __fadd_rn(g, ep.D[static_cast<size_t>(i) * ep.ldd + j]);
             }
@@ -364,7 +369,7 @@ __global__ void __launch_bounds__(kSpmmThreads, MINB) gradient_kernel(const int*
 // Fixed-point refresh of the structural term: the gather of gradient_kernel
 // (Y = B Tt = (A P B)^T over the tile), stored as Mq[i][j] = round(APB * scale)
 // in int64 (lane = j, so each store is a 256-byte row segment).  APB >= 0; a
-// value at or above 2^62 (or not finite) sets flags[1] and stores 0.
+// value at or above 2^52 (or not finite) sets flags[1] and stores 0.
 template <int U = 4>
 __global__ void __launch_bounds__(kSpmmThreads) structural_refresh_kernel(const int* __restrict__ rp,
                                                                           const int* __restrict__ col,
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(kSpmmThreads) structural_refresh_kernel(const 
             if (ib + t >= n) break;
             const double x = static_cast<double>(av[t]) * scale;
             long long m = 0;
-            if (x < 4611686018427387904.0 && x >= 0.0) m = __double2ll_rn(x);
+            if (x < 4503599627370496.0 && x >= 0.0) m = __double2ll_rn(x);
             else bad = true;
             Mq[row_offset(ib + t, ldm) + j] = m;
         }
@@ -398,129 +403,182 @@ __global__ void __launch_bounds__(kSpmmThreads) structural_refresh_kernel(const 
     if (bad) atomicOr(&flags[1], 1);
 }
 
+// (float)(m * scale) for a fixed-point value 0 <= m < 2^52: OR-ing m into the
+// mantissa of 2^52 gives the double 2^52 + m exactly, and one fused multiply-add,
+// (2^52 + m) scale - 2^52 scale, rounds m * scale once (no 64-bit integer
+// convert).
+__device__ __forceinline__ float fixed_to_float(long long m, double scale, double bias) {
+    const double x = __longlong_as_double(0x4330000000000000ll | m);
+    return __double2float_rn(fma(x, scale, bias));
+}
+
 // The gradient of gradient_kernel with APB read from the fixed-point structural
 // term (apb = (float)(Mq * m_scale)) instead of gathered: an elementwise pass.
-// CTA tile: 128 rows (i0 = 128 blockIdx.y, the column-statistics panel) x 128
-// columns (j0 = 128 blockIdx.x); lane l owns columns j0 + 4l .. j0 + 4l + 3 and
-// warp w the rows i0 + w + 8r, so every warp access is one contiguous row segment
-// (1 KB of Mq, 512 B of P and of out).  The per-column (max, sum) in base 2 is
-// kept online (one ex2 per element) and merged over the warps in shared memory.
-// SHIFT: Mq is also written back divided by 2^shift (rounded half up).
+// CTA tile: 128 rows (i0 = 128 blockIdx.y, the column-statistics panel) x 32 CPT
+// columns (j0 = 32 CPT blockIdx.x); lane l owns the CPT consecutive columns
+// j0 + CPT l ..., warp w the rows i0 + w + 8r, so every warp access is one
+// contiguous row segment (256 CPT bytes of Mq, 128 CPT of P and of the cost).
+// Each thread loads 8 / CPT rows before computing any of them (bytes in flight);
+// the tile's features and duals sit in shared memory.  The per-column (max, sum)
+// in base 2 is kept online (one ex2 per element) and merged over the warps in
+// shared memory.  SHIFT: Mq is also written back divided by 2^shift (rounded
+// half up).  SQ: the distance's square root as sqrt.approx, as gradient_kernel's.
 constexpr int kStructThreads = 256;
 constexpr int kStructRows = 128;
-constexpr int kStructCols = 128;
+// 2 columns per thread: 4 columns (2 rows in flight, 3 CTAs per SM) measured
+// 4.13 against 3.91 ms per FW step at n = 32768
+constexpr int kStructCpt = 2;
 
-template <bool COLSTATS, bool SHIFT>
-__global__ void __launch_bounds__(kStructThreads) gradient_structural_kernel(long long* __restrict__ Mq,
-                                                                              long long ldm, double m_scale,
-                                                                              int shift, int n,
-                                                                              const EpilogueArgs ep) {
+template <int CPT> struct StructVec;
+template <> struct StructVec<2> {
+    static __device__ __forceinline__ void load_m(const long long* p, long long (&m)[2]) {
+        const longlong2 a = *reinterpret_cast<const longlong2*>(p);
+        m[0] = a.x;
+        m[1] = a.y;
+    }
+    static __device__ __forceinline__ void load_p(const float* p, float (&v)[2]) {
+        const float2 a = *reinterpret_cast<const float2*>(p);
+        v[0] = a.x;
+        v[1] = a.y;
+    }
+    static __device__ __forceinline__ void store_o(float* p, const float (&o)[2]) {
+        *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
+    }
+    static __device__ __forceinline__ void store_m(long long* p, const long long (&m)[2]) {
+        *reinterpret_cast<longlong2*>(p) = make_longlong2(m[0], m[1]);
+    }
+};
+template <bool COLSTATS, bool SHIFT, bool SQ, int CPT>
+__global__ void __launch_bounds__(kStructThreads, 4) gradient_structural_kernel(
+    long long* __restrict__ Mq, long long ldm, double m_scale, int shift, int n, const EpilogueArgs ep) {
     constexpr int kWarps = kStructThreads / 32;
-    __shared__ float2 cst[COLSTATS ? kWarps : 1][kStructCols];
+    constexpr int kCols = 32 * CPT;
+    constexpr int kBatch = 8 / CPT;
+    constexpr int kRowsPerWarp = kStructRows / kWarps;
+    using Vec = StructVec<CPT>;
+    __shared__ float4 s_fs[kStructRows];
+    __shared__ double s_u[kStructRows];
+    __shared__ float4 s_ft[kCols];
+    __shared__ double s_v[kCols];
+    __shared__ float2 cst[COLSTATS ? kWarps : 1][kCols];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int j0 = blockIdx.x * kStructCols;
+    const int j0 = blockIdx.x * kCols;
     const int i0 = blockIdx.y * kStructRows;
-    const int jb = j0 + 4 * lane;
+    const int jb = j0 + CPT * lane;
     const bool has_f = ep.fs != nullptr;
     const bool has_d = !has_f && ep.D != nullptr;
     const float lam = static_cast<float>(ep.lam);
     const bool use_p = lam != 0.f;
-    const bool full = jb + 3 < n;
-    float4 f2[4];
-    double vj[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int j = jb + c;
-        f2[c] = (has_f && j < n) ? reinterpret_cast<const float4*>(ep.ft)[j] : make_float4(0, 0, 0, 0);
-        vj[c] = (ep.V != nullptr && j < n) ? ep.V[j] : 0.0;
+    const double m_bias = -4503599627370496.0 * m_scale;
+    for (int t = threadIdx.x; t < kStructRows; t += kStructThreads) {
+        const int i = i0 + t;
+        s_fs[t] = (has_f && i < n) ? reinterpret_cast<const float4*>(ep.fs)[i] : make_float4(0, 0, 0, 0);
+        s_u[t] = (ep.U != nullptr && i < n) ? ep.U[i] : 0.0;
     }
-    float cm[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
-    float cs[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int t = threadIdx.x; t < kCols; t += kStructThreads) {
+        const int j = j0 + t;
+        s_ft[t] = (has_f && j < n) ? reinterpret_cast<const float4*>(ep.ft)[j] : make_float4(0, 0, 0, 0);
+        s_v[t] = (ep.V != nullptr && j < n) ? ep.V[j] : 0.0;
+    }
+    __syncthreads();
+    const bool full = jb + CPT - 1 < n;
+    float cm[CPT], cs[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        cm[c] = -INFINITY;
+        cs[c] = 0.f;
+    }
     const long long half = SHIFT ? (1ll << (shift - 1)) : 0;
     if (jb < n) {
-#pragma unroll 2
-        for (int r = 0; r < kStructRows / kWarps; ++r) {
-            const int i = i0 + warp + kWarps * r;
-            if (i >= n) break;
-            long long* mrow = Mq + row_offset(i, ldm) + jb;
-            long long m[4];
-            float p[4] = {0.f, 0.f, 0.f, 0.f};
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
-            if (full) {
-                const longlong2 a = *reinterpret_cast<const longlong2*>(mrow);
-                const longlong2 b = *reinterpret_cast<const longlong2*>(mrow + 2);
-                m[0] = a.x; m[1] = a.y; m[2] = b.x; m[3] = b.y;
-                if (use_p) {
-                    const float4 p4 = *reinterpret_cast<const float4*>(ep.P + row_offset(i, ep.ldp) + jb);
-                    p[0] = p4.x; p[1] = p4.y; p[2] = p4.z; p[3] = p4.w;
-                }
-            } else {
+        for (int r0 = 0; r0 < kRowsPerWarp; r0 += kBatch) {
+            long long m[kBatch][CPT];
+            float p[kBatch][CPT];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    m[c] = jb + c < n ? mrow[c] : 0;
-                    if (use_p && jb + c < n) p[c] = ep.P[row_offset(i, ep.ldp) + jb + c];
-                }
-            }
-            if (has_d) {
+            for (int b = 0; b < kBatch; ++b) {
+                const int i = i0 + warp + kWarps * (r0 + b);
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    if (jb + c < n) d[c] = ep.D[row_offset(i, ep.ldd) + jb + c];
-            }
-            const double ui = ep.U ? ep.U[i] : 0.0;
-            const float4 f1 = has_f ? reinterpret_cast<const float4*>(ep.fs)[i] : make_float4(0, 0, 0, 0);
-            float o[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const float apb = __double2float_rn(__ll2double_rn(m[c]) * m_scale);
-                // the FP32 gradient in the order of gradient_kernel's scalar path
-                float reg = 0.f;
-                if (use_p) reg = __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, p[c])));
-                float g = __fadd_rn(__fmul_rn(-2.0f, apb), reg);
-                if (has_f) {
-                    const float d0 = __fsub_rn(f1.x, f2[c].x), d1 = __fsub_rn(f1.y, f2[c].y);
-                    const float d2 = __fsub_rn(f1.z, f2[c].z), d3 = __fsub_rn(f1.w, f2[c].w);
-                    g = __fadd_rn(g, __fsqrt_rn(__fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))))));
-                } else if (has_d) {
-                    g = __fadd_rn(g, d[c]);
+                for (int c = 0; c < CPT; ++c) {
+                    m[b][c] = 0;
+                    p[b][c] = 0.f;
                 }
-                o[c] = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + vj[c]));
-                if (COLSTATS && jb + c < n) {
-                    const float x = o[c] * kLog2e;
-                    if (x > cm[c]) {
-                        cs[c] = fmaf(cs[c], ex2(cm[c] - x), 1.0f);
-                        cm[c] = x;
-                    } else {
-                        cs[c] += ex2(x - cm[c]);
+                if (i >= n) continue;
+                const long long* mrow = Mq + row_offset(i, ldm) + jb;
+                const float* prow = ep.P + row_offset(i, ep.ldp) + jb;
+                if (full) {
+                    Vec::load_m(mrow, m[b]);
+                    if (use_p) Vec::load_p(prow, p[b]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < CPT; ++c) {
+                        if (jb + c >= n) break;
+                        m[b][c] = mrow[c];
+                        if (use_p) p[b][c] = prow[c];
                     }
                 }
             }
-            float* orow = ep.out + row_offset(i, ep.ldo) + jb;
-            if (full) {
-                *reinterpret_cast<float4*>(orow) = make_float4(o[0], o[1], o[2], o[3]);
-            } else {
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    if (jb + c < n) orow[c] = o[c];
-            }
-            if constexpr (SHIFT) {
+            for (int b = 0; b < kBatch; ++b) {
+                const int ii = warp + kWarps * (r0 + b);
+                const int i = i0 + ii;
+                if (i >= n) break;
+                const double ui = s_u[ii];
+                const float4 f1 = s_fs[ii];
+                float o[CPT];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) m[c] = (m[c] + half) >> shift;
+                for (int c = 0; c < CPT; ++c) {
+                    const float apb = fixed_to_float(m[b][c], m_scale, m_bias);
+                    // the FP32 gradient in the order of gradient_kernel's scalar path
+                    float reg = 0.f;
+                    if (use_p) reg = __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, p[b][c])));
+                    float g = __fadd_rn(__fmul_rn(-2.0f, apb), reg);
+                    if (has_f) {
+                        const float4 f2 = s_ft[CPT * lane + c];
+                        const float d0 = __fsub_rn(f1.x, f2.x), d1 = __fsub_rn(f1.y, f2.y);
+                        const float d2 = __fsub_rn(f1.z, f2.z), d3 = __fsub_rn(f1.w, f2.w);
+                        const float ss = __fmaf_rn(d3, d3, __fmaf_rn(d2, d2, __fmaf_rn(d1, d1, __fmul_rn(d0, d0))));
+                        float dist;
+                        if constexpr (SQ) asm("sqrt.approx.f32 %0, %1;" : "=f"(dist) : "f"(ss));
+                        else dist = __fsqrt_rn(ss);
+                        g = __fadd_rn(g, dist);
+                    } else if (has_d && jb + c < n) {
+                        g = __fadd_rn(g, ep.D[row_offset(i, ep.ldd) + jb + c]);
+                    }
+                    o[c] = static_cast<float>(ep.out_scale * static_cast<double>(g) + (ui + s_v[CPT * lane + c]));
+                    if (COLSTATS && (full || jb + c < n)) {
+                        const float x = o[c] * kLog2e;
+                        if (x > cm[c]) {
+                            cs[c] = fmaf(cs[c], ex2(cm[c] - x), 1.0f);
+                            cm[c] = x;
+                        } else {
+                            cs[c] += ex2(x - cm[c]);
+                        }
+                    }
+                }
+                float* orow = ep.out + row_offset(i, ep.ldo) + jb;
+                long long* mrow = Mq + row_offset(i, ldm) + jb;
+                if constexpr (SHIFT) {
+#pragma unroll
+                    for (int c = 0; c < CPT; ++c) m[b][c] = (m[b][c] + half) >> shift;
+                }
                 if (full) {
-                    reinterpret_cast<longlong2*>(mrow)[0] = make_longlong2(m[0], m[1]);
-                    reinterpret_cast<longlong2*>(mrow)[1] = make_longlong2(m[2], m[3]);
+                    Vec::store_o(orow, o);
+                    if constexpr (SHIFT) Vec::store_m(mrow, m[b]);
                 } else {
 #pragma unroll
-                    for (int c = 0; c < 4; ++c)
-                        if (jb + c < n) mrow[c] = m[c];
+                    for (int c = 0; c < CPT; ++c) {
+                        if (jb + c >= n) break;
+                        orow[c] = o[c];
+                        if constexpr (SHIFT) mrow[c] = m[b][c];
+                    }
                 }
             }
         }
     }
     if constexpr (COLSTATS) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) cst[warp][4 * lane + c] = make_float2(cm[c], cs[c]);
+        for (int c = 0; c < CPT; ++c) cst[warp][CPT * lane + c] = make_float2(cm[c], cs[c]);
         __syncthreads();
-        if (threadIdx.x < kStructCols && j0 + static_cast<int>(threadIdx.x) < n) {
+        if (threadIdx.x < kCols && j0 + static_cast<int>(threadIdx.x) < n) {
             const int t = threadIdx.x;
             float M = -INFINITY;
 #pragma unroll
@@ -561,9 +619,12 @@ int gather_unroll() {
     const char* e = getenv("FUGAL_GATHER_UNROLL");
     return (e != nullptr && atoi(e) == 8) ? 8 : 4;
 }
+// The distance's square root: sqrt.approx by default, the rounding of the
+// reference's distance kernel (built with --use_fast_math, cuda_kernels/setup.py:19);
+// FUGAL_GRAD_SQRT_APPROX=0 takes the IEEE-rounded square root.
 bool gradient_sqrt_approx() {
     const char* e = getenv("FUGAL_GRAD_SQRT_APPROX");
-    return e != nullptr && atoi(e) != 0;
+    return !(e != nullptr && atoi(e) == 0);
 }
 bool gradient_packed() {
     const char* e = getenv("FUGAL_GRAD_PACKED");
@@ -688,7 +749,10 @@ fugal_status fw_gradient(int64_t n, const int32_t* a_row_pointers, const int32_t
             else
                 gradient_kernel<true, 4, 6><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
         } else {
-            gradient_kernel<false, 4, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
+            if (gradient_sqrt_approx())
+                gradient_kernel<false, 4, 8, true, true><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
+            else
+                gradient_kernel<false, 4, 8><<<grid, kSpmmThreads, 0, stream>>>(brp, bci, Tt, ldt, ni, ep);
         }
         FUGAL_TRY(launch_check("fugal_fw_gradient: (A P) B + epilogue"));
     }
@@ -792,18 +856,23 @@ extern "C" fugal_status fugal_fw_gradient_structural(int64_t n, int64_t* Mq_, in
     if (shift < 0 || shift > 62) return fail(FUGAL_BAD_ARGUMENT, "%s: shift must be in [0, 62]", who);
     EpilogueArgs ep{P,   ldp, source_features, target_features, D, ldd, lambda * lambda_scale, out_scale, U, V, out,
                     ldo, reinterpret_cast<float2*>(column_partials), ldc};
-    dim3 grid(static_cast<unsigned>((n + kStructCols - 1) / kStructCols),
-              static_cast<unsigned>((n + kStructRows - 1) / kStructRows));
+    const int cols = 32 * kStructCpt;
+    dim3 grid(static_cast<unsigned>((n + cols - 1) / cols), static_cast<unsigned>((n + kStructRows - 1) / kStructRows));
     const int ni = static_cast<int>(n);
     long long* Mq = reinterpret_cast<long long*>(Mq_);
     LaunchScope scope(FUGAL_KERNEL_GRADIENT, stream);
-    if (column_partials != nullptr && shift > 0)
-        gradient_structural_kernel<true, true><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, shift, ni, ep);
-    else if (column_partials != nullptr)
-        gradient_structural_kernel<true, false><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, 0, ni, ep);
-    else if (shift > 0)
-        gradient_structural_kernel<false, true><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, shift, ni, ep);
-    else
-        gradient_structural_kernel<false, false><<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, 0, ni, ep);
+    const bool sq = gradient_sqrt_approx();
+    auto launch = [&](auto colstats, auto shifted, auto approx) {
+        constexpr bool C = decltype(colstats)::value, S = decltype(shifted)::value, Q = decltype(approx)::value;
+        gradient_structural_kernel<C, S, Q, kStructCpt>
+            <<<grid, kStructThreads, 0, stream>>>(Mq, ldm, m_scale, shift, ni, ep);
+    };
+    using T = std::true_type;
+    using F = std::false_type;
+    const bool cp = column_partials != nullptr, sh = shift > 0;
+    if (cp && sh) { if (sq) launch(T{}, T{}, T{}); else launch(T{}, T{}, F{}); }
+    else if (cp)  { if (sq) launch(T{}, F{}, T{}); else launch(T{}, F{}, F{}); }
+    else if (sh)  { if (sq) launch(F{}, T{}, T{}); else launch(F{}, T{}, F{}); }
+    else          { if (sq) launch(F{}, F{}, T{}); else launch(F{}, F{}, F{}); }
     return launch_check(who);
 }

@@ -43,7 +43,7 @@ ROW_SUM_BITS = 5            # log2(ROW_SUM_MAX)
 SCALE_BITS = 8              # scale stays >= 2^-SCALE_BITS between rescales
 RESCALE_BELOW = 2.0 ** -6   # rescale Mq by a power of two once scale drops below this
 MIN_FRAC_BITS = 24          # fewer fraction bits than this: keep the SpMM gradient
-VALUE_BITS = 62             # |Mq| < 2^62
+VALUE_BITS = 52             # 0 <= Mq < 2^52: its double is exact and cheap to form
 
 
 def frac_bits(max_degree: int) -> int:
@@ -51,7 +51,7 @@ def frac_bits(max_degree: int) -> int:
 
     ``M[i][j] <= deg_A(i) * max row sum of P <= max_degree * ROW_SUM_MAX`` and
     ``Mq = M / scale * 2^F`` with ``scale >= 2^-SCALE_BITS``, so
-    ``Mq < 2^62`` when ``F = 62 - SCALE_BITS - ROW_SUM_BITS - ceil(log2(max_degree + 1))``."""
+    ``Mq < 2^52`` when ``F = 52 - SCALE_BITS - ROW_SUM_BITS - ceil(log2(max_degree + 1))``."""
     if max_degree < 0:
         raise ValueError("max_degree must be >= 0")
     return VALUE_BITS - SCALE_BITS - ROW_SUM_BITS - math.ceil(math.log2(max_degree + 1))
@@ -132,6 +132,7 @@ class StructuralTerm:
         self.Mq = torch.empty((self.n, self.ld), dtype=torch.int64, device=dev)
         self.counts = torch.zeros(self.n, dtype=torch.int32, device=dev)
         self.entries = torch.zeros((self.n, SLOTS, 2), dtype=torch.int32, device=dev)
+        # [a plan row was not added, the fixed-point range was exceeded]
         self.flags = torch.zeros(2, dtype=torch.int32, device=dev)
         self.a_nnz = int(self.A.col_indices.numel())
         self.edge_rows = torch.empty(max(1, self.a_nnz), dtype=torch.int32, device=dev)

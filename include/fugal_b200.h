@@ -377,7 +377,7 @@ fugal_status fugal_fw_update(int64_t n, float* P, int64_t ldp, const float* cost
  * and frac_bits held by the caller.  A step only adds to the entries that A q B
  * touches; integer addition is associative, so the sums do not depend on the
  * order of the atomic adds and reruns are bit-identical.  Choose frac_bits so
- * that d_max * FUGAL_PLAN_ROW_SUM_MAX * 2^frac_bits / scale < 2^62, d_max the
+ * that d_max * FUGAL_PLAN_ROW_SUM_MAX * 2^frac_bits / scale < 2^52, d_max the
  * largest degree of A, for every scale used between refreshes.
  *
  * flags: two device int32, zeroed by the caller.  flags[0] != 0: the scatter
@@ -396,7 +396,7 @@ fugal_status fugal_csr_edge_rows(const int32_t* row_pointers, int64_t n, int64_t
                                  fugal_stream_t stream);
 
 /* Mq[i][j] = round((A P B)[i][j] * 2^frac_bits) for i, j < n (the SpMM pair of
- * fugal_fw_gradient, same workspace); flags[1] is set on a value >= 2^62. */
+ * fugal_fw_gradient, same workspace); flags[1] is set on a value >= 2^52. */
 fugal_status fugal_structural_refresh(int64_t n, const int32_t* a_row_pointers, const int32_t* a_col_indices,
                                       const int32_t* b_row_pointers, const int32_t* b_col_indices, const float* P,
                                       int64_t ldp, int64_t* Mq, int64_t ldm, int32_t frac_bits, void* workspace,

@@ -15,14 +15,14 @@ import pytest
 from cugal_b200 import structural as S
 
 
-def test_frac_bits_keep_values_below_2_62():
+def test_frac_bits_keep_values_below_2_52():
     for d in [0, 1, 2, 15, 16, 17, 1000, 65535]:
         F = S.frac_bits(d)
         bound = d * S.ROW_SUM_MAX * 2.0 ** F * 2.0 ** S.SCALE_BITS
-        assert bound < 2.0 ** 62, (d, F)
-        # one bit fewer of headroom would already allow more than 2^62 for some degree
-        assert (2 ** math.ceil(math.log2(d + 1))) * S.ROW_SUM_MAX * 2.0 ** (F + S.SCALE_BITS) <= 2.0 ** 62
-    assert S.frac_bits(16) == 62 - 8 - 5 - 5
+        assert bound < 2.0 ** 52, (d, F)
+        # the bound is tight: the next power of two of the degree reaches 2^52 exactly
+        assert (2 ** math.ceil(math.log2(d + 1))) * S.ROW_SUM_MAX * 2.0 ** (F + S.SCALE_BITS) == 2.0 ** 52
+    assert S.frac_bits(16) == 52 - 8 - 5 - 5
     with pytest.raises(ValueError):
         S.frac_bits(-1)
 
@@ -86,7 +86,7 @@ def _simulate(n, g, h, plans, alphas, seed):
             inc = int(np.rint(q[kk, l] * factor))
             for i in a_ci[a_rp[kk]:a_rp[kk + 1]]:
                 Mq[i, b_ci[b_rp[l]:b_rp[l + 1]]] += inc
-        assert Mq.max() < 2 ** 62 and Mq.min() >= 0
+        assert Mq.max() < 2 ** 52 and Mq.min() >= 0
     M = Mq.astype(np.float64) * fp.m_scale()
     worst = max(worst, float(np.max(np.abs(M - A @ P @ B))))
     return worst, fp
