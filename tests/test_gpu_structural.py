@@ -213,3 +213,58 @@ def test_kept_term_reruns_are_bit_identical(monkeypatch):
     assert eng1.structural.scatters > 0
     assert torch.equal(eng1.P, eng2.P)
     assert torch.equal(eng1.structural.Mq, eng2.structural.Mq)
+
+
+@pytest.mark.parametrize("n", [250, 384])
+@pytest.mark.parametrize("distance", ["features", "stored", "none"])
+@pytest.mark.parametrize("partials", [True, False])
+def test_structural_gradient_equals_spmm_gradient(n, distance, partials):
+    """Every form of the kept-term gradient against the SpMM gradient of the same
+    dyadic P, bit for bit: the distance from features, from a stored matrix, or
+    none; with and without column partials; n not a multiple of the tiles (250)."""
+    from cugal_b200 import _native as N
+    A, B, ld, ws, st, P = _setup(n, seed=n)
+    P[:, :n] = 1.0 / 256
+    rng = np.random.default_rng(n)
+    assert st.prepare(P)
+    z32 = torch.zeros(ld, dtype=torch.float32, device="cuda")
+    z64 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    gap = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        st.collect_update(P, _plan_cost(n, ld, rng, extra_rows=range(1, n - 1, 13)), z32, z32, z64, z64, 0.5, 1e-3,
+                          gap)
+    torch.cuda.synchronize()
+    assert st.flags.tolist() == [0, 0]
+    fs = ft = D = None
+    if distance == "features":
+        fs = torch.tensor(rng.random((n, 4)) * 3, dtype=torch.float32, device="cuda")
+        ft = torch.tensor(rng.random((n, 4)) * 3, dtype=torch.float32, device="cuda")
+    elif distance == "stored":
+        D = torch.zeros((n, ld), dtype=torch.float32, device="cuda")
+        D[:, :n] = torch.tensor(rng.random((n, n)) * 5, dtype=torch.float32, device="cuda")
+    U = torch.tensor(rng.standard_normal(n) * 1e3, device="cuda")
+    V = torch.tensor(rng.standard_normal(n) * 1e3, device="cuda")
+    chunks = (n + 127) // 128
+    out_d = torch.zeros((n, ld), dtype=torch.float32, device="cuda")
+    out_s = torch.zeros_like(out_d)
+    part_d = torch.zeros((chunks, 2 * ld), dtype=torch.float32, device="cuda")
+    part_s = torch.zeros_like(part_d)
+    stream = N.stream_handle("cuda")
+    dist_args = (N.ptr(fs), N.ptr(ft), N.ptr(D), ld if D is not None else 0)
+    common = (*dist_args, 3.0, 1.0, -1e3, U.data_ptr(), V.data_ptr())
+    graphs = (A.row_pointers.data_ptr(), A.col_indices.data_ptr(), B.row_pointers.data_ptr(),
+              B.col_indices.data_ptr(), P.data_ptr(), ld)
+    if partials:
+        N.call("fugal_fw_gradient_column_stats", n, *graphs, *common, out_d.data_ptr(), ld, ws.data_ptr(),
+               ws.numel(), part_d.data_ptr(), ld, stream)
+    else:
+        N.call("fugal_fw_gradient", n, *graphs, *common, out_d.data_ptr(), ld, ws.data_ptr(), ws.numel(), stream)
+    N.call("fugal_fw_gradient_structural", n, st.Mq.data_ptr(), ld, st.fixed.m_scale(), 0, P.data_ptr(), ld,
+           *common, out_s.data_ptr(), ld, part_s.data_ptr() if partials else None, ld, stream)
+    torch.cuda.synchronize()
+    assert torch.equal(out_s[:, :n], out_d[:, :n])
+    if partials:
+        pd = part_d.view(chunks, ld, 2)[:, :n]
+        ps = part_s.view(chunks, ld, 2)[:, :n]
+        assert torch.equal(ps[..., 0], pd[..., 0])
+        torch.testing.assert_close(ps[..., 1], pd[..., 1], rtol=2e-5, atol=0)
