@@ -96,3 +96,44 @@ def test_ctypes_structs_match_c_layout(cls, struct):
     assert layout[0] == ctypes.sizeof(cls)
     for name, off in zip(names, layout[1:]):
         assert getattr(cls, name).offset == off, name
+
+
+def declared_arities() -> dict[str, int]:
+    """Parameter count of every function the header declares."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(fugal_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_signatures_have_the_header_arities():
+    arities = declared_arities()
+    assert set(arities) == set(N.SIGNATURES), set(arities) ^ set(N.SIGNATURES)
+    wrong = {name: (arities[name], len(args)) for name, (_, args) in N.SIGNATURES.items()
+             if arities[name] != len(args)}
+    assert not wrong, wrong
+
+
+def test_plan_entry_layout_matches_header():
+    # the plan slots are read on the host as int32 pairs (column, float bits)
+    assert _c_layout("fugal_plan_entry", ["column", "value"]) == [8, 0, 4]
+
+
+@pytest.mark.parametrize("call", [
+    lambda: N.call("fugal_csr_edge_rows", None, 10, 5, None, None),
+    lambda: N.call("fugal_structural_refresh", 16, None, None, None, None, None, 16, None, 16, 30, None, 0, None,
+                   None),
+    lambda: N.call("fugal_structural_scatter", 16, None, None, 5, None, None, None, None, 32, 1.0, None, 16, None,
+                   None),
+    lambda: N.call("fugal_structural_scatter", 0, None, None, 5, None, None, None, None, 32, 1.0, None, 16, None,
+                   None),
+    lambda: N.call("fugal_fw_gradient_structural", 16, None, 16, 1.0, 0, None, 16, None, None, None, 0, 0.0, 1.0,
+                   -1.0, None, None, None, 16, None, 16, None),
+    lambda: N.call("fugal_fw_update_collect", 16, None, 16, None, 16, None, None, None, None, 0.5, 1.0, None, 0,
+                   None, None, 32, None),
+])
+def test_kept_term_entry_points_reject_bad_arguments_before_launch(call):
+    with pytest.raises(N.NativeError):
+        call()
